@@ -1,0 +1,321 @@
+"""bmfr_b200 — B200 (sm_100a) implementation of the BMFR per-frame denoising
+pipeline (Blockwise Multi-Order Feature Regression, opencl/bmfr.cl).
+
+The five stages keep the reference kernels' names and argument lists
+(accumulate_noisy_data, fitter, weighted_sum, accumulate_filtered_data, taa);
+``Plan`` also runs the reference host program's frame loop
+(opencl/bmfr.cpp:417-485) on plan-owned history buffers.  All compute is in
+the native library libbmfr_b200.so; torch is used only to hold device memory
+and to name CUDA streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native
+from ._native import (BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check, lib,
+                      PIPELINE_FUSED, PIPELINE_STAGED)
+
+__all__ = [
+    "Plan", "Scene", "BmfrError", "default_params", "block_offsets",
+    "accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa",
+    "PIPELINE_FUSED", "PIPELINE_STAGED", "library_path",
+]
+
+library_path = _native.library_path
+
+
+def default_params(**overrides) -> Params:
+    """The reference's compile-time options (opencl/bmfr.cpp:56-118) as a Params."""
+    p = Params()
+    check(lib.bmfr_params_default(C.byref(p)), "bmfr_params_default")
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"unknown BMFR parameter {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def block_offsets() -> np.ndarray:
+    """BLOCK_OFFSETS (opencl/bmfr.cl:267-285) as a (16, 2) int array."""
+    out = (C.c_int * 32)()
+    check(lib.bmfr_block_offsets(out), "bmfr_block_offsets")
+    return np.array(out, dtype=np.int32).reshape(16, 2)
+
+
+def _stream_ptr(stream) -> C.c_void_p:
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _ptr(t, name: str, nbytes: int | None = None, optional: bool = False) -> C.c_void_p:
+    """Device pointer of a contiguous CUDA tensor (or None)."""
+    if t is None:
+        if optional:
+            return C.c_void_p(None)
+        raise ValueError(f"{name} must not be None")
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if nbytes is not None and t.numel() * t.element_size() < nbytes:
+        raise ValueError(f"{name} holds {t.numel() * t.element_size()} bytes, needs {nbytes}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _f32(values, n: int, name: str):
+    a = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+    if a.size != n:
+        raise ValueError(f"{name} needs {n} floats")
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Plan:
+    """Sizes of one image stream plus the frame pipeline's history buffers.
+
+    ``Plan(1280, 720)`` uses the reference's defaults; keyword arguments
+    override fields of Params (e.g. ``pipeline=PIPELINE_STAGED``).
+    """
+
+    def __init__(self, width: int, height: int, params: Params | None = None, **overrides):
+        self.params = params if params is not None else default_params(**overrides)
+        h = C.c_void_p()
+        check(lib.bmfr_plan_create(C.byref(self.params), int(width), int(height), C.byref(h)),
+              "bmfr_plan_create")
+        self._h = h
+        s = Sizes()
+        check(lib.bmfr_plan_sizes(h, C.byref(s)), "bmfr_plan_sizes")
+        self.sizes = s
+        self.width, self.height = s.image_width, s.image_height
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if self._h is None:
+            raise BmfrError(_native.BMFR_E_STATE, "plan destroyed")
+        return self._h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            lib.bmfr_plan_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- frame pipeline (opencl/bmfr.cpp:417-485) --------------------------
+    @property
+    def frame_number(self) -> int:
+        return lib.bmfr_plan_frame_number(self.handle)
+
+    def frame_inputs(self) -> FrameInputs:
+        fi = FrameInputs()
+        check(lib.bmfr_plan_frame_inputs(self.handle, C.byref(fi)), "bmfr_plan_frame_inputs")
+        return fi
+
+    def upload_frame(self, albedo, normals, positions, noisy, stream=None) -> None:
+        """Copies one frame's four host buffers (float32, H*W*3) into the plan."""
+        arrs = []
+        n = self.width * self.height * 3
+        for name, a in (("albedo", albedo), ("normals", normals), ("positions", positions), ("noisy", noisy)):
+            if hasattr(a, "data_ptr"):
+                if a.is_cuda or a.numel() != n or a.dtype.itemsize != 4 or not a.is_contiguous():
+                    raise ValueError(f"{name}: contiguous float32 host tensor of {n} values expected")
+                arrs.append(C.c_void_p(a.data_ptr()))
+            else:
+                a = np.ascontiguousarray(a, dtype=np.float32)
+                if a.size != n:
+                    raise ValueError(f"{name}: {n} values expected")
+                arrs.append(C.c_void_p(a.ctypes.data))
+        check(lib.bmfr_plan_upload_frame(self.handle, *arrs, _stream_ptr(stream)), "bmfr_plan_upload_frame")
+
+    def denoise_frame(self, prev_frame_camera_matrix, pixel_offset, stream=None) -> None:
+        """Runs the five stages for the next frame and swaps the histories."""
+        m, mp = _f32(prev_frame_camera_matrix, 16, "prev_frame_camera_matrix")
+        o, op = _f32(pixel_offset, 2, "pixel_offset")
+        check(lib.bmfr_denoise_frame(self.handle, mp, op, _stream_ptr(stream)), "bmfr_denoise_frame")
+
+    def denoise_frame_io(self, albedo, normals, positions, noisy, previous_normals, previous_positions,
+                         prev_frame_camera_matrix, pixel_offset, result=None, stream=None) -> None:
+        """denoise_frame on caller-owned device tensors (float32, H*W*3)."""
+        n = self.width * self.height * 12
+        first = self.frame_number == 0
+        io = FrameIO(_ptr(albedo, "albedo", n), _ptr(normals, "normals", n), _ptr(positions, "positions", n),
+                     _ptr(noisy, "noisy", n), _ptr(previous_normals, "previous_normals", n, optional=first),
+                     _ptr(previous_positions, "previous_positions", n, optional=first),
+                     _ptr(result, "result", n, optional=True))
+        m, mp = _f32(prev_frame_camera_matrix, 16, "prev_frame_camera_matrix")
+        o, op = _f32(pixel_offset, 2, "pixel_offset")
+        check(lib.bmfr_denoise_frame_io(self.handle, C.byref(io), mp, op, _stream_ptr(stream)),
+              "bmfr_denoise_frame_io")
+
+    def result_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.bmfr_plan_result(self.handle, C.byref(p)), "bmfr_plan_result")
+        return p.value
+
+    def download_result(self, out=None, stream=None) -> np.ndarray:
+        """Copies the last TAA output to host memory (blocking unless `out`
+        is a pinned tensor and a stream is given)."""
+        if out is None:
+            out = np.empty((self.height, self.width, 3), dtype=np.float32)
+            check(lib.bmfr_plan_download_result(self.handle, C.c_void_p(out.ctypes.data), _stream_ptr(stream)),
+                  "bmfr_plan_download_result")
+            import torch
+            torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+            return out
+        check(lib.bmfr_plan_download_result(self.handle, C.c_void_p(out.data_ptr()), _stream_ptr(stream)),
+              "bmfr_plan_download_result")
+        return out
+
+    def buffers(self) -> PlanBuffers:
+        b = PlanBuffers()
+        check(lib.bmfr_plan_buffers_get(self.handle, C.byref(b)), "bmfr_plan_buffers_get")
+        return b
+
+    def reset(self) -> None:
+        check(lib.bmfr_plan_reset(self.handle), "bmfr_plan_reset")
+
+
+# -- the five stages (drop-in for opencl/bmfr.cl's kernels) ------------------
+
+def accumulate_noisy_data(plan: Plan, out_prev_frame_pixel, accept_bools, current_normals, previous_normals,
+                          current_positions, previous_positions, current_noisy, previous_noisy, previous_spp,
+                          current_spp, tmp_data, prev_frame_camera_matrix, pixel_offset, frame_number: int,
+                          stream=None) -> None:
+    """opencl/bmfr.cl:290-485; current_noisy is updated in place."""
+    px = plan.width * plan.height
+    hist = frame_number > 0
+    m, mp = _f32(prev_frame_camera_matrix, 16, "prev_frame_camera_matrix")
+    o, op = _f32(pixel_offset, 2, "pixel_offset")
+    check(lib.bmfr_accumulate_noisy_data(
+        plan.handle, _ptr(out_prev_frame_pixel, "out_prev_frame_pixel", px * 8),
+        _ptr(accept_bools, "accept_bools", px), _ptr(current_normals, "current_normals", px * 12),
+        _ptr(previous_normals, "previous_normals", px * 12, optional=not hist),
+        _ptr(current_positions, "current_positions", px * 12),
+        _ptr(previous_positions, "previous_positions", px * 12, optional=not hist),
+        _ptr(current_noisy, "current_noisy", px * 12),
+        _ptr(previous_noisy, "previous_noisy", px * 12, optional=not hist),
+        _ptr(previous_spp, "previous_spp", px, optional=not hist), _ptr(current_spp, "current_spp", px),
+        _ptr(tmp_data, "tmp_data", plan.sizes.tmp_data_bytes), mp, op, int(frame_number),
+        _stream_ptr(stream)), "accumulate_noisy_data")
+
+
+def fitter(plan: Plan, weights, mins_maxs, tmp_data, frame_number: int, stream=None) -> None:
+    """opencl/bmfr.cl:490-700."""
+    check(lib.bmfr_fitter(plan.handle, _ptr(weights, "weights", plan.sizes.weights_bytes),
+                          _ptr(mins_maxs, "mins_maxs", plan.sizes.mins_maxs_bytes),
+                          _ptr(tmp_data, "tmp_data", plan.sizes.tmp_data_bytes), int(frame_number),
+                          _stream_ptr(stream)), "fitter")
+
+
+def weighted_sum(plan: Plan, weights, mins_maxs, output, current_normals, current_positions, current_noisy,
+                 frame_number: int, stream=None) -> None:
+    """opencl/bmfr.cl:703-758 (current_noisy is unused, as in the reference)."""
+    px = plan.width * plan.height
+    check(lib.bmfr_weighted_sum(plan.handle, _ptr(weights, "weights", plan.sizes.weights_bytes),
+                                _ptr(mins_maxs, "mins_maxs", plan.sizes.mins_maxs_bytes),
+                                _ptr(output, "output", px * 12), _ptr(current_normals, "current_normals", px * 12),
+                                _ptr(current_positions, "current_positions", px * 12),
+                                _ptr(current_noisy, "current_noisy", optional=True), int(frame_number),
+                                _stream_ptr(stream)), "weighted_sum")
+
+
+def accumulate_filtered_data(plan: Plan, filtered_frame, in_prev_frame_pixel, accept_bools, albedo,
+                             tone_mapped_frame, current_spp, accumulated_prev_frame, accumulated_frame,
+                             frame_number: int, stream=None) -> None:
+    """opencl/bmfr.cl:761-857."""
+    px = plan.width * plan.height
+    hist = frame_number > 0
+    check(lib.bmfr_accumulate_filtered_data(
+        plan.handle, _ptr(filtered_frame, "filtered_frame", px * 12),
+        _ptr(in_prev_frame_pixel, "in_prev_frame_pixel", px * 8, optional=not hist),
+        _ptr(accept_bools, "accept_bools", px, optional=not hist), _ptr(albedo, "albedo", px * 12),
+        _ptr(tone_mapped_frame, "tone_mapped_frame", px * 12),
+        _ptr(current_spp, "current_spp", px, optional=not hist),
+        _ptr(accumulated_prev_frame, "accumulated_prev_frame", px * 12, optional=not hist),
+        _ptr(accumulated_frame, "accumulated_frame", px * 12), int(frame_number), _stream_ptr(stream)),
+        "accumulate_filtered_data")
+
+
+def taa(plan: Plan, in_prev_frame_pixel, new_frame, result_frame, prev_frame, frame_number: int,
+        stream=None) -> None:
+    """opencl/bmfr.cl:860-974."""
+    px = plan.width * plan.height
+    check(lib.bmfr_taa(plan.handle, _ptr(in_prev_frame_pixel, "in_prev_frame_pixel", px * 8),
+                       _ptr(new_frame, "new_frame", px * 12), _ptr(result_frame, "result_frame", px * 12),
+                       _ptr(prev_frame, "prev_frame", px * 12, optional=frame_number == 0), int(frame_number),
+                       _stream_ptr(stream)), "taa")
+
+
+# -- input source ------------------------------------------------------------
+
+class Scene:
+    """Seeded procedural stand-in for the reference's EXR dataset and
+    camera_matrices.h (opencl/bmfr.cpp:44-53, 145-172)."""
+
+    def __init__(self, seed: int, width: int, height: int, sphere_count: int = 12, **overrides):
+        d = SceneDesc()
+        check(lib.bmfr_scene_default(C.byref(d), int(seed), int(width), int(height), int(sphere_count)),
+              "bmfr_scene_default")
+        for k, v in overrides.items():
+            if not hasattr(d, k):
+                raise AttributeError(f"unknown scene field {k!r}")
+            setattr(d, k, v)
+        self.desc = d
+        self.width, self.height = width, height
+
+    @property
+    def position_limit_squared(self) -> float:
+        return self.desc.position_limit_squared
+
+    @property
+    def normal_limit_squared(self) -> float:
+        return self.desc.normal_limit_squared
+
+    def camera(self, frame: int) -> np.ndarray:
+        m = np.empty(16, dtype=np.float32)
+        check(lib.bmfr_scene_camera(C.byref(self.desc), int(frame), m.ctypes.data_as(C.POINTER(C.c_float))),
+              "bmfr_scene_camera")
+        return m
+
+    def prev_camera(self, frame: int) -> np.ndarray:
+        """camera_matrices[max(frame - 1, 0)], the matrix frame `frame` uses
+        (opencl/bmfr.cpp:440-442)."""
+        return self.camera(max(frame - 1, 0))
+
+    def pixel_offset(self, frame: int) -> np.ndarray:
+        o = np.empty(2, dtype=np.float32)
+        check(lib.bmfr_scene_pixel_offset(C.byref(self.desc), int(frame), o.ctypes.data_as(C.POINTER(C.c_float))),
+              "bmfr_scene_pixel_offset")
+        return o
+
+    def render(self, frame: int, clean: bool = False, threads: int = 0) -> dict:
+        H, W = self.height, self.width
+        out = {k: np.empty((H, W, 3), dtype=np.float32) for k in ("albedo", "normals", "positions", "noisy")}
+        cl = np.empty((H, W, 3), dtype=np.float32) if clean else None
+        fp = C.POINTER(C.c_float)
+        check(lib.bmfr_scene_render(C.byref(self.desc), int(frame), out["albedo"].ctypes.data_as(fp),
+                                    out["normals"].ctypes.data_as(fp), out["positions"].ctypes.data_as(fp),
+                                    out["noisy"].ctypes.data_as(fp),
+                                    cl.ctypes.data_as(fp) if cl is not None else None, int(threads)),
+              "bmfr_scene_render")
+        if cl is not None:
+            out["clean"] = cl
+        return out

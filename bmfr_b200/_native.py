@@ -1,0 +1,148 @@
+"""ctypes binding of libbmfr_b200.so (include/bmfr_b200.h, include/bmfr_scene.h).
+
+The library is the product: importing this module loads it and raises if it
+is missing — there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "libbmfr_b200.so"
+
+BMFR_OK = 0
+BMFR_E_INVALID = -1
+BMFR_E_CUDA = -2
+BMFR_E_UNSUPPORTED = -3
+BMFR_E_NOMEM = -4
+BMFR_E_BUDGET = -5
+BMFR_E_NOT_FOUND = -6
+BMFR_E_AGAIN = -7
+BMFR_E_TIMEOUT = -8
+BMFR_E_STATE = -9
+BMFR_E_TOO_LARGE = -10
+
+PIPELINE_STAGED = 0
+PIPELINE_FUSED = 1
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("noise_amount", C.c_double),
+        ("blend_alpha", C.c_float),
+        ("second_blend_alpha", C.c_float),
+        ("taa_blend_alpha", C.c_float),
+        ("position_limit_squared", C.c_float),
+        ("normal_limit_squared", C.c_float),
+        ("use_half_precision_in_tmp_data", C.c_int),
+        ("compressed_r", C.c_int),
+        ("cache_tmp_data", C.c_int),
+        ("fp32_qr", C.c_int),
+        ("half_history", C.c_int),
+        ("pipeline", C.c_int),
+    ]
+
+
+class Sizes(C.Structure):
+    _fields_ = [
+        ("image_width", C.c_int), ("image_height", C.c_int),
+        ("workset_width", C.c_int), ("workset_height", C.c_int),
+        ("margin_width", C.c_int), ("margin_height", C.c_int),
+        ("blocks_x", C.c_int), ("blocks_y", C.c_int), ("blocks", C.c_int),
+        ("tmp_data_bytes", C.c_size_t), ("weights_bytes", C.c_size_t),
+        ("mins_maxs_bytes", C.c_size_t), ("pixel3_bytes", C.c_size_t),
+    ]
+
+
+class FrameInputs(C.Structure):
+    _fields_ = [("albedo", C.c_void_p), ("normals", C.c_void_p),
+                ("positions", C.c_void_p), ("noisy", C.c_void_p)]
+
+
+class PlanBuffers(C.Structure):
+    _fields_ = [("tmp_data", C.c_void_p), ("weights", C.c_void_p), ("mins_maxs", C.c_void_p),
+                ("filtered", C.c_void_p), ("prev_frame_pixel", C.c_void_p),
+                ("tone_mapped", C.c_void_p), ("accept", C.c_void_p), ("spp", C.c_void_p),
+                ("accumulated_noisy", C.c_void_p), ("accumulated_filtered", C.c_void_p),
+                ("result", C.c_void_p)]
+
+
+class FrameIO(C.Structure):
+    _fields_ = [("albedo", C.c_void_p), ("normals", C.c_void_p), ("positions", C.c_void_p),
+                ("noisy", C.c_void_p), ("previous_normals", C.c_void_p),
+                ("previous_positions", C.c_void_p), ("result", C.c_void_p)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("width", C.c_int), ("height", C.c_int),
+        ("sphere_count", C.c_int), ("orbit_degrees_per_frame", C.c_float),
+        ("orbit_start_degrees", C.c_float), ("orbit_radius", C.c_float),
+        ("camera_height", C.c_float), ("vertical_fov_degrees", C.c_float),
+        ("noise_mu", C.c_float), ("noise_sigma", C.c_float),
+        ("firefly_fraction", C.c_float), ("firefly_scale", C.c_float),
+        ("plane_half_extent", C.c_float), ("position_limit_squared", C.c_float),
+        ("normal_limit_squared", C.c_float),
+    ]
+
+
+def _load() -> C.CDLL:
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python bmfr_b200/build.py` "
+            "(the CUDA library is required; there is no CPU fallback)")
+    lib = C.CDLL(str(_LIB_PATH))
+    vp, i, f, fp, u8p = C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_float), C.c_void_p
+    sig = {
+        "bmfr_params_default": (i, [C.POINTER(Params)]),
+        "bmfr_plan_create": (i, [C.POINTER(Params), i, i, C.POINTER(vp)]),
+        "bmfr_plan_destroy": (i, [vp]),
+        "bmfr_plan_sizes": (i, [vp, C.POINTER(Sizes)]),
+        "bmfr_plan_params": (i, [vp, C.POINTER(Params)]),
+        "bmfr_block_offsets": (i, [C.POINTER(C.c_int)]),
+        "bmfr_accumulate_noisy_data": (i, [vp, vp, u8p, vp, vp, vp, vp, vp, vp, u8p, u8p, vp, fp, fp, i, vp]),
+        "bmfr_fitter": (i, [vp, vp, vp, vp, i, vp]),
+        "bmfr_weighted_sum": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp]),
+        "bmfr_accumulate_filtered_data": (i, [vp, vp, vp, u8p, vp, vp, u8p, vp, vp, i, vp]),
+        "bmfr_taa": (i, [vp, vp, vp, vp, vp, i, vp]),
+        "bmfr_plan_frame_inputs": (i, [vp, C.POINTER(FrameInputs)]),
+        "bmfr_plan_upload_frame": (i, [vp, vp, vp, vp, vp, vp]),
+        "bmfr_denoise_frame": (i, [vp, fp, fp, vp]),
+        "bmfr_denoise_frame_io": (i, [vp, C.POINTER(FrameIO), fp, fp, vp]),
+        "bmfr_plan_result": (i, [vp, C.POINTER(vp)]),
+        "bmfr_plan_download_result": (i, [vp, vp, vp]),
+        "bmfr_plan_frame_number": (i, [vp]),
+        "bmfr_plan_reset": (i, [vp]),
+        "bmfr_plan_buffers_get": (i, [vp, C.POINTER(PlanBuffers)]),
+        "bmfr_last_error": (C.c_char_p, []),
+        "bmfr_status_string": (C.c_char_p, [i]),
+        "bmfr_scene_default": (i, [C.POINTER(SceneDesc), C.c_uint64, i, i, i]),
+        "bmfr_scene_camera": (i, [C.POINTER(SceneDesc), i, fp]),
+        "bmfr_scene_pixel_offset": (i, [C.POINTER(SceneDesc), i, fp]),
+        "bmfr_scene_render": (i, [C.POINTER(SceneDesc), i, fp, fp, fp, fp, fp, i]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class BmfrError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib.bmfr_last_error().decode()
+        super().__init__(f"{where}: {lib.bmfr_status_string(status).decode()} ({status}): {msg}")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != BMFR_OK:
+        raise BmfrError(status, where)
+
+
+def library_path() -> str:
+    return os.fspath(_LIB_PATH)

@@ -1,0 +1,456 @@
+// capi.cu — the C ABI of include/bmfr_b200.h: parameter checks, the plan
+// (sizes plus the frame pipeline's history buffers) and the launches.
+//
+// The plan mirrors the reference host program's buffer set and frame loop
+// (opencl/bmfr.cpp:315-347, 417-485): six double-buffered histories swapped
+// after every frame and eight single buffers, all resident in HBM.
+#include "bmfr_b200.h"
+#include "kernels.h"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(BMFR_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+struct bmfr_plan {
+    bmfr_params p;
+    bmfr::Geometry g;
+    int device = 0;
+    int frame = 0;
+    // Frame-pipeline buffers (bmfr.cpp:315-347).
+    float* normals[2] = {nullptr, nullptr};
+    float* positions[2] = {nullptr, nullptr};
+    float* albedo = nullptr;
+    float* noisy_in = nullptr;        // this frame's 1-spp colour
+    float* noisy_acc[2] = {nullptr, nullptr};   // accumulated noisy history
+    uint8_t* spp[2] = {nullptr, nullptr};
+    void* tmp = nullptr;
+    float* weights = nullptr;
+    float* mins_maxs = nullptr;
+    float* filtered = nullptr;
+    float2* prev_pix = nullptr;
+    uint8_t* accept = nullptr;
+    float* tone_mapped = nullptr;
+    void* acc_filt[2] = {nullptr, nullptr};     // accumulated filtered history
+    void* result[2] = {nullptr, nullptr};       // TAA history
+    float* result_f32 = nullptr;                // fp32 output when histories are binary16
+    const float* last_result = nullptr;         // float32 output of the last frame
+    std::vector<void*> allocations;
+};
+
+namespace {
+
+bool check_device(const bmfr_plan* plan) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    return dev == plan->device;
+}
+
+int check_plan(const bmfr_plan* plan) {
+    if (!plan) return fail(BMFR_E_INVALID, "plan is NULL");
+    if (!check_device(plan)) return fail(BMFR_E_STATE, "the current CUDA device is not the plan's device");
+    return BMFR_OK;
+}
+
+size_t pixel3_bytes(const bmfr_plan* p, bool half) {
+    return (size_t)p->g.W * p->g.H * 3 * (half ? 2 : 4);
+}
+
+size_t tmp_bytes(const bmfr::Geometry& g, bool half) {
+    return (size_t)g.MW * g.MH * bmfr::kBuffers * (half ? 2 : 4);
+}
+
+bmfr::AccumArgs accum_args(const bmfr_plan* plan, const float* m, const float* off, int frame) {
+    bmfr::AccumArgs a;
+    std::memcpy(a.m, m, sizeof a.m);
+    a.off_x = off[0];
+    a.off_y = off[1];
+    a.pos_lim2 = plan->p.position_limit_squared;
+    a.nrm_lim2 = plan->p.normal_limit_squared;
+    a.blend_alpha = plan->p.blend_alpha;
+    a.frame = frame;
+    a.use_half = plan->p.use_half_precision_in_tmp_data ? 1 : 0;
+    return a;
+}
+
+void free_plan(bmfr_plan* plan) {
+    for (void* p : plan->allocations) cudaFree(p);
+    delete plan;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bmfr_last_error(void) { return g_last_error.c_str(); }
+
+const char* bmfr_status_string(int status) {
+    switch (status) {
+        case BMFR_OK: return "ok";
+        case BMFR_E_INVALID: return "invalid argument";
+        case BMFR_E_CUDA: return "CUDA error";
+        case BMFR_E_UNSUPPORTED: return "unsupported parameter";
+        case BMFR_E_NOMEM: return "out of device memory";
+        case BMFR_E_BUDGET: return "over the memory budget";
+        case BMFR_E_NOT_FOUND: return "not found";
+        case BMFR_E_AGAIN: return "not ready";
+        case BMFR_E_TIMEOUT: return "timed out";
+        case BMFR_E_STATE: return "invalid state";
+        case BMFR_E_TOO_LARGE: return "size beyond the fixed maximum";
+        default: return "unknown status";
+    }
+}
+
+int bmfr_params_default(bmfr_params* p) {
+    if (!p) return fail(BMFR_E_INVALID, "params is NULL");
+    std::memset(p, 0, sizeof *p);
+    p->noise_amount = 1e-2;            // bmfr.cpp:58
+    p->blend_alpha = 0.2f;             // bmfr.cpp:60
+    p->second_blend_alpha = 0.1f;      // bmfr.cpp:61
+    p->taa_blend_alpha = 0.2f;         // bmfr.cpp:62
+    p->position_limit_squared = 0.01f; // dataset-defined in the reference
+    p->normal_limit_squared = 0.1f;
+    p->use_half_precision_in_tmp_data = 1;   // bmfr.cpp:88
+    p->compressed_r = 1;               // bmfr.cpp:82
+    p->cache_tmp_data = 1;             // bmfr.cpp:84
+    p->fp32_qr = 0;
+    p->half_history = 0;
+    p->pipeline = BMFR_PIPELINE_FUSED;
+    return BMFR_OK;
+}
+
+int bmfr_block_offsets(int out_xy[32]) {
+    static const int t[32] = {-14, -14, 4, -6, -8, 14, 8, 0, -10, -8, 2, 12, 12, -12, -10, 0,
+                              12, 14, -8, -16, 6, 6, -2, -2, 6, -14, -16, 12, 14, -4, -6, 4};
+    if (!out_xy) return fail(BMFR_E_INVALID, "out_xy is NULL");
+    std::memcpy(out_xy, t, sizeof t);
+    return BMFR_OK;
+}
+
+int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan** out) {
+    if (!params || !out) return fail(BMFR_E_INVALID, "params/plan pointer is NULL");
+    *out = nullptr;
+    if (width < 32 || height < 32 || width > 16384 || height > 16384)
+        return fail(BMFR_E_INVALID, "image size must be within [32, 16384]");
+    const bmfr::Geometry g = bmfr::make_geometry(width, height);
+    // mirror() (bmfr.cl:209-216) must stay within one image size: the margin
+    // grid reaches WORKSET + 29 on the right/bottom and -32 on the left/top.
+    if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
+        return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
+    if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    if (params->pipeline != BMFR_PIPELINE_STAGED && params->pipeline != BMFR_PIPELINE_FUSED)
+        return fail(BMFR_E_INVALID, "unknown pipeline");
+    if (!(params->blend_alpha > 0.f) || !(params->second_blend_alpha > 0.f))
+        return fail(BMFR_E_INVALID, "blend factors must be positive");
+    int device = -1;
+    if (cudaError_t e = cudaGetDevice(&device); e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "no CUDA device");
+    }
+    bmfr_plan* plan = new bmfr_plan;
+    plan->p = *params;
+    plan->g = g;
+    plan->device = device;
+    const bool half_tmp = params->use_half_precision_in_tmp_data != 0;
+    const bool half_hist = params->half_history != 0;
+    const size_t px = (size_t)width * height;
+    auto alloc = [&](size_t bytes, auto** ptr) -> bool {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cudaMemset(p, 0, bytes);
+        plan->allocations.push_back(p);
+        *ptr = static_cast<std::remove_pointer_t<decltype(ptr)>>(p);
+        return true;
+    };
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) {
+        ok = ok && alloc(px * 12, &plan->normals[i]) && alloc(px * 12, &plan->positions[i]) &&
+             alloc(px * 12, &plan->noisy_acc[i]) && alloc(px, &plan->spp[i]) &&
+             alloc(pixel3_bytes(plan, half_hist), &plan->acc_filt[i]) &&
+             alloc(pixel3_bytes(plan, half_hist), &plan->result[i]);
+    }
+    ok = ok && alloc(px * 12, &plan->albedo) && alloc(px * 12, &plan->noisy_in) &&
+         alloc(tmp_bytes(g, half_tmp), &plan->tmp) &&
+         alloc((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &plan->weights) &&
+         alloc((size_t)g.blocks * bmfr::kScaled * 2 * 4, &plan->mins_maxs) &&
+         alloc(px * 12, &plan->filtered) && alloc(px * 8, &plan->prev_pix) && alloc(px, &plan->accept) &&
+         alloc(px * 12, &plan->tone_mapped);
+    if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32);
+    if (!ok) {
+        free_plan(plan);
+        return fail(BMFR_E_NOMEM, "device allocation for the plan failed");
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        free_plan(plan);
+        return cuda_fail(e, "plan initialisation");
+    }
+    *out = plan;
+    return BMFR_OK;
+}
+
+int bmfr_plan_destroy(bmfr_plan* plan) {
+    if (!plan) return BMFR_OK;
+    free_plan(plan);
+    return BMFR_OK;
+}
+
+int bmfr_plan_sizes(const bmfr_plan* plan, bmfr_sizes* s) {
+    if (!plan || !s) return fail(BMFR_E_INVALID, "NULL argument");
+    const bmfr::Geometry& g = plan->g;
+    s->image_width = g.W;
+    s->image_height = g.H;
+    s->workset_width = g.MW - 32;
+    s->workset_height = g.MH - 32;
+    s->margin_width = g.MW;
+    s->margin_height = g.MH;
+    s->blocks_x = g.MWb;
+    s->blocks_y = g.MHb;
+    s->blocks = g.blocks;
+    s->tmp_data_bytes = tmp_bytes(g, plan->p.use_half_precision_in_tmp_data != 0);
+    s->weights_bytes = (size_t)g.blocks * bmfr::kFeatures * 3 * sizeof(float);
+    s->mins_maxs_bytes = (size_t)g.blocks * bmfr::kScaled * 2 * sizeof(float);
+    s->pixel3_bytes = (size_t)g.W * g.H * 3 * sizeof(float);
+    return BMFR_OK;
+}
+
+int bmfr_plan_params(const bmfr_plan* plan, bmfr_params* p) {
+    if (!plan || !p) return fail(BMFR_E_INVALID, "NULL argument");
+    *p = plan->p;
+    return BMFR_OK;
+}
+
+int bmfr_accumulate_noisy_data(const bmfr_plan* plan, float* out_prev_frame_pixel, uint8_t* accept_bools,
+                               const float* current_normals, const float* previous_normals,
+                               const float* current_positions, const float* previous_positions,
+                               float* current_noisy, const float* previous_noisy, const uint8_t* previous_spp,
+                               uint8_t* current_spp, void* tmp_data, const float* prev_frame_camera_matrix,
+                               const float* pixel_offset, int frame_number, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!out_prev_frame_pixel || !accept_bools || !current_normals || !current_positions || !current_noisy ||
+        !current_spp || !tmp_data || !prev_frame_camera_matrix || !pixel_offset)
+        return fail(BMFR_E_INVALID, "accumulate_noisy_data: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "accumulate_noisy_data: negative frame number");
+    if (frame_number > 0 && (!previous_normals || !previous_positions || !previous_noisy || !previous_spp))
+        return fail(BMFR_E_INVALID, "accumulate_noisy_data: NULL history buffer");
+    const bmfr::AccumArgs a = accum_args(plan, prev_frame_camera_matrix, pixel_offset, frame_number);
+    cudaError_t e = bmfr::launch_accumulate_noisy(
+        plan->g, a, reinterpret_cast<float2*>(out_prev_frame_pixel), accept_bools, current_normals,
+        previous_normals, current_positions, previous_positions, current_noisy, current_noisy, previous_noisy,
+        previous_spp, current_spp, tmp_data, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "accumulate_noisy_data launch");
+}
+
+int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const void* tmp_data, int frame_number,
+                void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!weights || !mins_maxs || !tmp_data) return fail(BMFR_E_INVALID, "fitter: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter: negative frame number");
+    cudaError_t e = bmfr::launch_fitter(plan->g, frame_number, bmfr::make_noise_const(plan->p.noise_amount),
+                                        tmp_data, plan->p.use_half_precision_in_tmp_data != 0,
+                                        plan->p.fp32_qr != 0, weights, mins_maxs, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
+}
+
+int bmfr_weighted_sum(const bmfr_plan* plan, const float* weights, const float* mins_maxs, float* output,
+                      const float* current_normals, const float* current_positions, const float* current_noisy,
+                      int frame_number, void* stream) {
+    (void)current_noisy;   // debug-only in the reference (bmfr.cl:709, 752-754)
+    if (int st = check_plan(plan)) return st;
+    if (!weights || !mins_maxs || !output || !current_normals || !current_positions)
+        return fail(BMFR_E_INVALID, "weighted_sum: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "weighted_sum: negative frame number");
+    cudaError_t e = bmfr::launch_weighted_sum(plan->g, frame_number, weights, mins_maxs, output, current_normals,
+                                              current_positions, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "weighted_sum launch");
+}
+
+int bmfr_accumulate_filtered_data(const bmfr_plan* plan, const float* filtered_frame,
+                                  const float* in_prev_frame_pixel, const uint8_t* accept_bools,
+                                  const float* albedo, float* tone_mapped_frame, const uint8_t* current_spp,
+                                  const float* accumulated_prev_frame, float* accumulated_frame, int frame_number,
+                                  void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!filtered_frame || !albedo || !tone_mapped_frame || !accumulated_frame)
+        return fail(BMFR_E_INVALID, "accumulate_filtered_data: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "accumulate_filtered_data: negative frame number");
+    if (frame_number > 0 && (!in_prev_frame_pixel || !accept_bools || !current_spp || !accumulated_prev_frame))
+        return fail(BMFR_E_INVALID, "accumulate_filtered_data: NULL history buffer");
+    cudaError_t e = bmfr::launch_accumulate_filtered(
+        plan->g, frame_number, plan->p.second_blend_alpha, filtered_frame,
+        reinterpret_cast<const float2*>(in_prev_frame_pixel), accept_bools, albedo, tone_mapped_frame,
+        current_spp, accumulated_prev_frame, accumulated_frame, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "accumulate_filtered_data launch");
+}
+
+int bmfr_taa(const bmfr_plan* plan, const float* in_prev_frame_pixel, const float* new_frame, float* result_frame,
+             const float* prev_frame, int frame_number, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!in_prev_frame_pixel || !new_frame || !result_frame) return fail(BMFR_E_INVALID, "taa: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "taa: negative frame number");
+    if (frame_number > 0 && !prev_frame) return fail(BMFR_E_INVALID, "taa: NULL history buffer");
+    cudaError_t e = bmfr::launch_taa(plan->g, frame_number, plan->p.taa_blend_alpha,
+                                     reinterpret_cast<const float2*>(in_prev_frame_pixel), new_frame, result_frame,
+                                     prev_frame, nullptr, false, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "taa launch");
+}
+
+// ---- plan-managed pipeline ------------------------------------------------
+
+int bmfr_plan_frame_inputs(bmfr_plan* plan, bmfr_frame_inputs* in) {
+    if (!plan || !in) return fail(BMFR_E_INVALID, "NULL argument");
+    const int cur = plan->frame & 1;
+    in->albedo = plan->albedo;
+    in->normals = plan->normals[cur];
+    in->positions = plan->positions[cur];
+    in->noisy = plan->noisy_in;
+    return BMFR_OK;
+}
+
+int bmfr_plan_upload_frame(bmfr_plan* plan, const float* albedo, const float* normals, const float* positions,
+                           const float* noisy, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!albedo || !normals || !positions || !noisy) return fail(BMFR_E_INVALID, "upload: NULL host buffer");
+    bmfr_frame_inputs in;
+    bmfr_plan_frame_inputs(plan, &in);
+    const size_t bytes = (size_t)plan->g.W * plan->g.H * 12;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(in.albedo, albedo, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in.normals, normals, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in.positions, positions, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in.noisy, noisy, bytes, cudaMemcpyHostToDevice, s);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "upload");
+}
+
+namespace {
+
+// One frame of the pipeline (bmfr.cpp:429-476) on the given inputs; the
+// histories are the plan's.  prev_n/prev_p may be null at frame 0.
+int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const float* prev_n, const float* cur_p,
+              const float* prev_p, const float* noisy, float* extra_result, const float* m, const float* off,
+              cudaStream_t s) {
+    const int f = plan->frame;
+    const int cur = f & 1, prv = cur ^ 1;
+    const bmfr::Geometry& g = plan->g;
+    const bool half_tmp = plan->p.use_half_precision_in_tmp_data != 0;
+    const bool half_hist = plan->p.half_history != 0;
+    if (f > 0 && (!prev_n || !prev_p)) return fail(BMFR_E_INVALID, "denoise_frame: previous G-buffer missing");
+    const bmfr::AccumArgs a = accum_args(plan, m, off, f);
+    cudaError_t e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
+                                                  noisy, plan->noisy_acc[cur], plan->noisy_acc[prv],
+                                                  plan->spp[prv], plan->spp[cur], plan->tmp, s);
+    if (e == cudaSuccess)
+        e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
+                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, s);
+    if (e == cudaSuccess) {
+        if (plan->p.pipeline == BMFR_PIPELINE_STAGED && !half_hist) {
+            e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
+            if (e == cudaSuccess)
+                e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered,
+                                                     plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
+                                                     plan->spp[cur], (const float*)plan->acc_filt[prv],
+                                                     (float*)plan->acc_filt[cur], s);
+        } else {
+            e = bmfr::launch_weighted_sum_accumulate(
+                g, f, plan->p.second_blend_alpha, plan->weights, plan->mins_maxs, cur_n, cur_p,
+                plan->p.pipeline == BMFR_PIPELINE_STAGED ? plan->filtered : nullptr, plan->prev_pix, plan->accept,
+                albedo, plan->tone_mapped, plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur], half_hist, s);
+        }
+    }
+    float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32 : nullptr);
+    if (e == cudaSuccess)
+        e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped, plan->result[cur],
+                             plan->result[prv], f32_out, half_hist, s);
+    if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
+    plan->last_result = half_hist ? f32_out : (const float*)plan->result[cur];
+    plan->frame = f + 1;   // swaps every double buffer (bmfr.cpp:482-484)
+    return BMFR_OK;
+}
+
+}  // namespace
+
+int bmfr_denoise_frame(bmfr_plan* plan, const float* prev_frame_camera_matrix, const float* pixel_offset,
+                       void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!prev_frame_camera_matrix || !pixel_offset) return fail(BMFR_E_INVALID, "denoise_frame: NULL matrix/offset");
+    const int cur = plan->frame & 1, prv = cur ^ 1;
+    return run_frame(plan, plan->albedo, plan->normals[cur], plan->normals[prv], plan->positions[cur],
+                     plan->positions[prv], plan->noisy_in, nullptr, prev_frame_camera_matrix, pixel_offset,
+                     (cudaStream_t)stream);
+}
+
+int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io, const float* prev_frame_camera_matrix,
+                          const float* pixel_offset, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!io || !prev_frame_camera_matrix || !pixel_offset)
+        return fail(BMFR_E_INVALID, "denoise_frame_io: NULL argument");
+    if (!io->albedo || !io->normals || !io->positions || !io->noisy)
+        return fail(BMFR_E_INVALID, "denoise_frame_io: NULL input buffer");
+    return run_frame(plan, io->albedo, io->normals, io->previous_normals, io->positions, io->previous_positions,
+                     io->noisy, io->result, prev_frame_camera_matrix, pixel_offset, (cudaStream_t)stream);
+}
+
+int bmfr_plan_result(const bmfr_plan* plan, const float** result) {
+    if (!plan || !result) return fail(BMFR_E_INVALID, "NULL argument");
+    if (plan->frame == 0) return fail(BMFR_E_STATE, "no frame has been denoised");
+    *result = plan->last_result;
+    return BMFR_OK;
+}
+
+int bmfr_plan_download_result(const bmfr_plan* plan, float* host_rgb, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!host_rgb) return fail(BMFR_E_INVALID, "download: NULL host buffer");
+    const float* r = nullptr;
+    if (int st = bmfr_plan_result(plan, &r)) return st;
+    cudaError_t e = cudaMemcpyAsync(host_rgb, r, (size_t)plan->g.W * plan->g.H * 12, cudaMemcpyDeviceToHost,
+                                    (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "download");
+}
+
+int bmfr_plan_frame_number(const bmfr_plan* plan) { return plan ? plan->frame : BMFR_E_INVALID; }
+
+int bmfr_plan_reset(bmfr_plan* plan) {
+    if (!plan) return fail(BMFR_E_INVALID, "plan is NULL");
+    plan->frame = 0;
+    plan->last_result = nullptr;
+    return BMFR_OK;
+}
+
+int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* b) {
+    if (!plan || !b) return fail(BMFR_E_INVALID, "NULL argument");
+    std::memset(b, 0, sizeof *b);
+    const int last = (plan->frame + 1) & 1;   // slot written by the last frame
+    const bool staged = plan->p.pipeline == BMFR_PIPELINE_STAGED;
+    b->tmp_data = plan->tmp;
+    b->weights = plan->weights;
+    b->mins_maxs = plan->mins_maxs;
+    b->filtered = staged ? plan->filtered : nullptr;
+    b->prev_frame_pixel = reinterpret_cast<const float*>(plan->prev_pix);
+    b->tone_mapped = plan->tone_mapped;
+    b->accept = plan->accept;
+    b->spp = plan->spp[last];
+    b->accumulated_noisy = plan->noisy_acc[last];
+    b->accumulated_filtered = plan->acc_filt[last];
+    b->result = plan->last_result;
+    return BMFR_OK;
+}
+
+}  // extern "C"

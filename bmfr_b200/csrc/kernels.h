@@ -1,0 +1,48 @@
+// kernels.h — host-side launchers of the sm_100a kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace bmfr {
+
+cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float2* prev_pix, uint8_t* accept,
+                                    const float* cur_n, const float* prev_n, const float* cur_p,
+                                    const float* prev_p, const float* noisy_in, float* noisy_out,
+                                    const float* prev_noisy, const uint8_t* prev_spp, uint8_t* cur_spp,
+                                    void* tmp, cudaStream_t s);
+
+cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
+                          bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s);
+
+cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,
+                                float* out, const float* cur_n, const float* cur_p, cudaStream_t s);
+
+cudaError_t launch_accumulate_filtered(const Geometry& g, int frame, float second_alpha, const float* filtered,
+                                       const float2* prev_pix, const uint8_t* accept, const float* albedo,
+                                       float* tone_mapped, const uint8_t* cur_spp, const float* acc_prev,
+                                       float* acc_cur, cudaStream_t s);
+
+cudaError_t launch_weighted_sum_accumulate(const Geometry& g, int frame, float second_alpha,
+                                           const float* weights, const float* mins_maxs, const float* cur_n,
+                                           const float* cur_p, float* filtered, const float2* prev_pix,
+                                           const uint8_t* accept, const float* albedo, float* tone_mapped,
+                                           const uint8_t* cur_spp, const void* acc_prev, void* acc_cur,
+                                           bool half_history, cudaStream_t s);
+
+cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const float2* prev_pix,
+                       const float* new_frame, void* result, const void* prev_frame, float* result_f32,
+                       bool half_history, cudaStream_t s);
+
+// NOISE_AMOUNT * 2 split into hi + lo floats.
+inline NoiseConst make_noise_const(double noise_amount) {
+    const double c = noise_amount * 2.0;
+    NoiseConst n;
+    n.hi = (float)c;
+    n.lo = (float)(c - (double)n.hi);
+    return n;
+}
+
+}  // namespace bmfr
