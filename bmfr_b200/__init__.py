@@ -184,6 +184,17 @@ class Plan:
               "bmfr_plan_download_result")
         return out
 
+    def enable_profiling(self, enable: bool = True) -> None:
+        check(lib.bmfr_plan_enable_profiling(self.handle, int(enable)), "bmfr_plan_enable_profiling")
+
+    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa")
+
+    def stage_times(self) -> dict:
+        """Milliseconds per stage of the last profiled frame."""
+        ms = (C.c_float * 5)()
+        check(lib.bmfr_plan_stage_times(self.handle, ms), "bmfr_plan_stage_times")
+        return dict(zip(self.STAGES, map(float, ms)))
+
     def buffers(self) -> PlanBuffers:
         b = PlanBuffers()
         check(lib.bmfr_plan_buffers_get(self.handle, C.byref(b)), "bmfr_plan_buffers_get")

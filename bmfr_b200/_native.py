@@ -115,6 +115,9 @@ def _load() -> C.CDLL:
         "bmfr_plan_frame_number": (i, [vp]),
         "bmfr_plan_reset": (i, [vp]),
         "bmfr_plan_buffers_get": (i, [vp, C.POINTER(PlanBuffers)]),
+        "bmfr_plan_enable_profiling": (i, [vp, i]),
+        "bmfr_plan_check_device": (i, [vp, vp]),
+        "bmfr_plan_stage_times": (i, [vp, fp]),
         "bmfr_last_error": (C.c_char_p, []),
         "bmfr_status_string": (C.c_char_p, [i]),
         "bmfr_scene_default": (i, [C.POINTER(SceneDesc), C.c_uint64, i, i, i]),

@@ -49,7 +49,11 @@ struct bmfr_plan {
     void* acc_filt[2] = {nullptr, nullptr};     // accumulated filtered history
     void* result[2] = {nullptr, nullptr};       // TAA history
     float* result_f32 = nullptr;                // fp32 output when histories are binary16
+    int* dev_status = nullptr;                  // device error word (bounded waits)
     const float* last_result = nullptr;         // float32 output of the last frame
+    bool profiling = false;
+    bool profiled_frame = false;
+    cudaEvent_t events[6] = {};                 // stage boundaries of the last frame
     std::vector<void*> allocations;
 };
 
@@ -89,6 +93,8 @@ bmfr::AccumArgs accum_args(const bmfr_plan* plan, const float* m, const float* o
 }
 
 void free_plan(bmfr_plan* plan) {
+    for (cudaEvent_t& e : plan->events)
+        if (e) cudaEventDestroy(e);
     for (void* p : plan->allocations) cudaFree(p);
     delete plan;
 }
@@ -194,6 +200,7 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
          alloc(px * 12, &plan->filtered) && alloc(px * 8, &plan->prev_pix) && alloc(px, &plan->accept) &&
          alloc(px * 12, &plan->tone_mapped);
     if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32);
+    if (ok) ok = alloc(sizeof(int), &plan->dev_status);
     if (!ok) {
         free_plan(plan);
         return fail(BMFR_E_NOMEM, "device allocation for the plan failed");
@@ -263,10 +270,13 @@ int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const v
                 void* stream) {
     if (int st = check_plan(plan)) return st;
     if (!weights || !mins_maxs || !tmp_data) return fail(BMFR_E_INVALID, "fitter: NULL buffer");
+    if (reinterpret_cast<uintptr_t>(tmp_data) % 16 != 0)
+        return fail(BMFR_E_INVALID, "fitter: tmp_data must be 16-byte aligned");
     if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter: negative frame number");
     cudaError_t e = bmfr::launch_fitter(plan->g, frame_number, bmfr::make_noise_const(plan->p.noise_amount),
                                         tmp_data, plan->p.use_half_precision_in_tmp_data != 0,
-                                        plan->p.fp32_qr != 0, weights, mins_maxs, (cudaStream_t)stream);
+                                        plan->p.fp32_qr != 0, weights, mins_maxs, plan->dev_status,
+                                        (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
 }
 
@@ -354,15 +364,25 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     const bool half_hist = plan->p.half_history != 0;
     if (f > 0 && (!prev_n || !prev_p)) return fail(BMFR_E_INVALID, "denoise_frame: previous G-buffer missing");
     const bmfr::AccumArgs a = accum_args(plan, m, off, f);
+    const bool prof = plan->profiling;
+    auto mark = [&](int i) {
+        if (prof) cudaEventRecord(plan->events[i], s);
+    };
+    mark(0);
     cudaError_t e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
                                                   noisy, plan->noisy_acc[cur], plan->noisy_acc[prv],
                                                   plan->spp[prv], plan->spp[cur], plan->tmp, s);
+    mark(1);
     if (e == cudaSuccess)
         e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
-                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, s);
+                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->dev_status, s);
+    mark(2);
+    bool split = false;
     if (e == cudaSuccess) {
         if (plan->p.pipeline == BMFR_PIPELINE_STAGED && !half_hist) {
+            split = true;
             e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
+            mark(3);
             if (e == cudaSuccess)
                 e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered,
                                                      plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
@@ -375,11 +395,15 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
                 albedo, plan->tone_mapped, plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur], half_hist, s);
         }
     }
+    if (!split) mark(3);
+    mark(4);
     float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32 : nullptr);
     if (e == cudaSuccess)
         e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped, plan->result[cur],
                              plan->result[prv], f32_out, half_hist, s);
+    mark(5);
     if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
+    plan->profiled_frame = prof;
     plan->last_result = half_hist ? f32_out : (const float*)plan->result[cur];
     plan->frame = f + 1;   // swaps every double buffer (bmfr.cpp:482-484)
     return BMFR_OK;
@@ -431,6 +455,45 @@ int bmfr_plan_reset(bmfr_plan* plan) {
     if (!plan) return fail(BMFR_E_INVALID, "plan is NULL");
     plan->frame = 0;
     plan->last_result = nullptr;
+    return BMFR_OK;
+}
+
+int bmfr_plan_check_device(const bmfr_plan* plan, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    int v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, plan->dev_status, sizeof v, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "check_device");
+    if (v != 0) {
+        cudaMemsetAsync(plan->dev_status, 0, sizeof(int), (cudaStream_t)stream);
+        cudaStreamSynchronize((cudaStream_t)stream);
+        return fail(BMFR_E_TIMEOUT, "a kernel's bounded wait ran out (device status " + std::to_string(v) + ")");
+    }
+    return BMFR_OK;
+}
+
+int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable) {
+    if (int st = check_plan(plan)) return st;
+    if (enable && !plan->events[0]) {
+        for (cudaEvent_t& e : plan->events) {
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return cuda_fail(r, "cudaEventCreate");
+        }
+    }
+    plan->profiling = enable != 0;
+    return BMFR_OK;
+}
+
+int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]) {
+    if (int st = check_plan(plan)) return st;
+    if (!ms) return fail(BMFR_E_INVALID, "ms is NULL");
+    if (!plan->profiled_frame) return fail(BMFR_E_STATE, "no profiled frame");
+    cudaError_t e = cudaEventSynchronize(plan->events[5]);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
+    for (int i = 0; i < BMFR_STAGE_COUNT; ++i) {
+        e = cudaEventElapsedTime(&ms[i], plan->events[i], plan->events[i + 1]);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+    }
     return BMFR_OK;
 }
 

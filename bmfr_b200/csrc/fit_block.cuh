@@ -4,20 +4,33 @@
 //
 // Layout.  Each thread is one of the reference's 256 work-items and owns the
 // same four pixels of the 32x32 block (rows id, id+256, id+512, id+768 of the
-// 1024x13 matrix).  The whole block stays in registers, t[13][4], through the
-// min/max scaling, the ten Householder reflections and their updates; tmp
-// data is never written back.  Work-item ids are assigned to lanes as
+// 1024x13 matrix).  The block stays in registers through the min/max
+// scaling, the ten Householder reflections and their updates, as binary16
+// pairs when the reference rounds every in-place store to half
+// (bmfr.cl:540, 651) — the packed conversion is that rounding — and as
+// floats otherwise.  tmp_data is never written back.  Work-item ids are
+// assigned to lanes as
 //     id = 8*warp + (lane & 7) + 64*(lane >> 3)
 // so that the first stage of the reference's reduction tree (ids i, i+64,
 // i+128, i+192, bmfr.cl:32-33) sits inside one warp and runs on shuffles.
 //
 // Reductions.  block_reduce evaluates parallel_reduction_sum/min/max
 // (bmfr.cl:25-87) over exactly the same tree, so the sums round exactly as
-// the reference's do, and batches V independent reductions behind one pair of
-// barriers: the twelve min/max values of the scaling step, and per column the
-// up to twelve dot products, which are independent once the Householder
-// vector is known.  A column costs two batched reductions (norm, dots) — four
-// barriers — where the reference spends three barriers per dot product.
+// the reference's do, and batches up to 12 independent reductions behind
+// one pair of barriers: the twelve min/max values of the scaling step, and
+// per column the up to twelve dot products, which are independent once the
+// Householder vector is known.  A column costs two batched reductions (norm,
+// dots) — four barriers — where the reference spends three per dot product.
+//
+// Columns run in a loop; after each column the register tile shifts down by
+// one column so that every index into it is a compile-time constant.
+//
+// Division.  The rank-one update divides by the column's |u|^2, which is the
+// same for the whole block.  Its correctly rounded reciprocal is formed once
+// and every quotient is taken with Markstein's correction step
+// (q = a*y; r = fma(-q, b, a); q' = fma(r, y, q)), which returns the
+// correctly rounded a/b for normal operands within 2^+-60; other operands
+// take a true division.
 //
 // The colour columns' own reflections (columns 10..12, bmfr.cl:549 with
 // col_limited = 10) only change rows >= 10, which neither the back
@@ -32,9 +45,10 @@ struct FitterSmem {
     float part[12 * 64];   // first-stage partial sums, 64 per batched value
     float out[12];         // reduction results
     float ucl;             // u[col] broadcast from its owner
+    int status;            // nonzero: a bounded wait ran out
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
-    float Rb[3][11][11];   // per-channel copy used by the back substitution
+    float Rb[3][11][12];   // per-channel copy used by the back substitution
 };
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -44,7 +58,6 @@ __device__ __forceinline__ int work_item_id() {
     return 8 * warp + (lane & 7) + 64 * (lane >> 3);
 }
 
-// OP: 0 sum, 1 min, 2 max.  Values [0, SPLIT) use OP_A, [SPLIT, V) use OP_B.
 template <int OP>
 __device__ __forceinline__ float rop(float a, float b) {
     if (OP == 0) return a + b;
@@ -52,49 +65,44 @@ __device__ __forceinline__ float rop(float a, float b) {
     return fmax_cl(a, b);
 }
 
-template <int V, int SPLIT, int OP_A, int OP_B>
-__device__ __forceinline__ void block_reduce(const float (&v)[V], FitterSmem& sm) {
+// Batched work-group reduction of n <= VMAX values per thread.  Values
+// [0, split) use OP_A, [split, n) use OP_B (0 sum, 1 min, 2 max).
+template <int VMAX, int OP_A, int OP_B>
+__device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int split, FitterSmem& sm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-    for (int i = 0; i < V; ++i) {
-        const float a = v[i];
-        const float b = __shfl_down_sync(kFull, a, 8);
-        const float c = __shfl_down_sync(kFull, a, 16);
-        const float d = __shfl_down_sync(kFull, a, 24);
-        float s1;
-        if (i < SPLIT) {
-            if (OP_A == 0) s1 = a + ((b + c) + d);          // bmfr.cl:33
-            else s1 = rop<OP_A>(rop<OP_A>(rop<OP_A>(a, b), c), d);   // bmfr.cl:52-53, 74-75
-        } else {
-            if (OP_B == 0) s1 = a + ((b + c) + d);
-            else s1 = rop<OP_B>(rop<OP_B>(rop<OP_B>(a, b), c), d);
+    for (int i = 0; i < VMAX; ++i) {
+        if (i < n) {
+            const float a = v[i];
+            const float b = __shfl_down_sync(kFull, a, 8);
+            const float c = __shfl_down_sync(kFull, a, 16);
+            const float d = __shfl_down_sync(kFull, a, 24);
+            const int op = i < split ? OP_A : OP_B;
+            float s1;
+            if (op == 0) s1 = a + ((b + c) + d);                               // bmfr.cl:33
+            else if (op == 1) s1 = fmin_cl(fmin_cl(fmin_cl(a, b), c), d);    // bmfr.cl:52-53
+            else s1 = fmax_cl(fmax_cl(fmax_cl(a, b), c), d);                 // bmfr.cl:74-75
+            if (lane < 8) sm.part[i * 64 + 8 * warp + lane] = s1;
         }
-        if (lane < 8) sm.part[i * 64 + 8 * warp + lane] = s1;
     }
     __syncthreads();
     // Stages 2 and 3: value vi is finished by the 8-lane group `lane >> 3` of
     // warp vi % 8; lane j of the group forms sum_vec[j] (bmfr.cl:35-37).
     const int vi = warp + 8 * (lane >> 3);
     const int j = lane & 7;
+    const int op = vi < split ? OP_A : OP_B;
     float s2 = 0.0f;
-    const bool first = vi < SPLIT;
-    if (vi < V) {
+    if (vi < n) {
         const float* p = sm.part + vi * 64 + j;
-        const int op = first ? OP_A : OP_B;
         if (op == 0) {
             float acc = p[8];
 #pragma unroll
             for (int m = 2; m < 8; ++m) acc = acc + p[8 * m];
             s2 = p[0] + acc;
-        } else if (op == 1) {
-            float acc = p[0];
-#pragma unroll
-            for (int m = 1; m < 8; ++m) acc = fmin_cl(acc, p[8 * m]);
-            s2 = acc;
         } else {
             float acc = p[0];
 #pragma unroll
-            for (int m = 1; m < 8; ++m) acc = fmax_cl(acc, p[8 * m]);
+            for (int m = 1; m < 8; ++m) acc = op == 1 ? fmin_cl(acc, p[8 * m]) : fmax_cl(acc, p[8 * m]);
             s2 = acc;
         }
     }
@@ -104,102 +112,191 @@ __device__ __forceinline__ void block_reduce(const float (&v)[V], FitterSmem& sm
 #pragma unroll
     for (int m = 1; m < 8; ++m) {
         const float x = __shfl_sync(kFull, s2, base + m);
-        const int op = first ? OP_A : OP_B;
         r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
     }
-    if (vi < V && j == 0) sm.out[vi] = r;
+    if (vi < n && j == 0) sm.out[vi] = r;
     __syncthreads();
 }
 
-template <bool ROUND>
-__device__ __forceinline__ float stq(float v) {
-    return ROUND ? round_half(v) : v;
-}
+// The block as held by one thread: four rows of the 13 columns.
+template <bool HALF>
+struct Tile;
 
-// One Householder column (bmfr.cl:549-655) for COL < 10, then the next.
-template <int COL, bool ROUND>
-struct QrColumn {
-    static __device__ __forceinline__ void run(float (&t)[kBuffers][4], int id, int frame, NoiseConst nc,
-                                               FitterSmem& sm) {
-        // Norm of rows >= COL+1 (bmfr.cl:553-569).
-        float nv[1];
-        {
-            float s = 0.0f;
+template <>
+struct Tile<true> {   // binary16 storage: every store rounds to nearest even
+    __half2 h[kBuffers][2];
+    __device__ __forceinline__ float2 get2(int k, int p) const { return __half22float2(h[k][p]); }
+    __device__ __forceinline__ void set2(int k, int p, float a, float b) { h[k][p] = __floats2half2_rn(a, b); }
+    __device__ __forceinline__ void shift() {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (id + kLocal * q >= COL + 1) s = s + t[COL][q] * t[COL][q];
-            nv[0] = s;
+        for (int k = 0; k < kBuffers - 1; ++k) {
+            h[k][0] = h[k + 1][0];
+            h[k][1] = h[k + 1][1];
         }
-        if (id == COL) sm.ucl = t[COL][0];
-        block_reduce<1, 1, 0, 0>(nv, sm);
-        const float norm2 = sm.out[0];
-        const float ucl = sm.ucl;
-        // Work-item COL's step (bmfr.cl:580-588), evaluated by everyone.
-        const float vl = sqrtf(norm2 + ucl * ucl);
-        const float ucl_new = ucl - vl;
-        const float uls = norm2 + ucl_new * ucl_new;
-        if (id < COL) sm.Rm[COL][id] = t[COL][0];
-        if (id == COL) sm.Rm[COL][COL] = vl;
-        float u[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) u[q] = t[COL][q];
-        if (id == COL) u[0] = ucl_new;
-
-        if (COL == 0) {   // noise on the first load of features 1..9 (bmfr.cl:625-627)
-#pragma unroll
-            for (int fb = 1; fb < kFeatures; ++fb)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) t[fb][q] = add_noise(t[fb][q], noise_index(id, q, fb, frame), nc);
-        }
-        // Dot products with every later column (bmfr.cl:606-638).
-        constexpr int V = kBuffers - 1 - COL;
-        float d[V];
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            float s = 0.0f;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (id + kLocal * q >= COL) s = s + t[COL + 1 + i][q] * u[q];
-            d[i] = s;
-        }
-        block_reduce<V, V, 0, 0>(d, sm);
-        // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-            const float dot = sm.out[i];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (id + kLocal * q >= COL)
-                    t[COL + 1 + i][q] = stq<ROUND>(t[COL + 1 + i][q] - ((2.0f * u[q]) * dot) / uls);
-        }
-        QrColumn<COL + 1, ROUND>::run(t, id, frame, nc, sm);
     }
 };
-template <bool ROUND>
-struct QrColumn<kFeatures, ROUND> {
-    static __device__ __forceinline__ void run(float (&)[kBuffers][4], int, int, NoiseConst, FitterSmem&) {}
+
+template <>
+struct Tile<false> {   // float storage: no intermediate rounding
+    float f[kBuffers][4];
+    __device__ __forceinline__ float2 get2(int k, int p) const { return make_float2(f[k][2 * p], f[k][2 * p + 1]); }
+    __device__ __forceinline__ void set2(int k, int p, float a, float b) {
+        f[k][2 * p] = a;
+        f[k][2 * p + 1] = b;
+    }
+    __device__ __forceinline__ void shift() {
+#pragma unroll
+        for (int k = 0; k < kBuffers - 1; ++k)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) f[k][q] = f[k + 1][q];
+    }
 };
 
+// value + NOISE_AMOUNT*2*r with r = random(i) - 0.5 already formed
+// (bmfr.cl:173-182), rounded once (see add_noise in common.cuh).
+__device__ __forceinline__ float add_noise_r(float value, float r, NoiseConst c) {
+    const float p = c.hi * r;
+    const float pe = __fmaf_rn(c.hi, r, -p);
+    const float pl = __fmaf_rn(c.lo, r, pe);
+    const float s = value + p;
+    const float bv = s - value;
+    const float se = (value - (s - bv)) + (p - bv);
+    return s + (se + pl);
+}
+
+// True division, kept out of line so that the rare slow case costs no code
+// at every call site.
+__device__ __noinline__ float div_slow(float a, float b) { return a / b; }
+
+// a / b correctly rounded, given y = RN(1/b) and fast = b within 2^+-60.
+__device__ __forceinline__ float div_by(float a, float b, float y, bool fast) {
+    const float q = a * y;
+    const float r = __fmaf_rn(-q, b, a);
+    const float q1 = __fmaf_rn(r, y, q);
+    const float aa = fabsf(a);
+    if (fast && aa >= 0x1p-60f && aa <= 0x1p60f) return q1;
+    if (a == 0.0f && fast) return a;   // +-0 / b, b > 0
+    return div_slow(a, b);
+}
+
+// Shared-memory table of the fitter's feature noise r = random(i) - 0.5 for
+// features 1..9 and this thread's four rows; the same for every block of a
+// frame (bmfr.cl:179-181 does not involve the block index).
+struct NoiseTable {
+    float r[kFeatures - 1][4][kLocal];
+};
+
+__device__ __forceinline__ void fill_noise_table(NoiseTable& nt, int frame) {
+    const int id = work_item_id();
+#pragma unroll
+    for (int fb = 1; fb < kFeatures; ++fb)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) nt.r[fb - 1][q][threadIdx.x] = hash_random(noise_index(id, q, fb, frame)) - 0.5f;
+}
+
+// One Householder column (bmfr.cl:549-655) on tile column 0; later columns
+// are tile columns 1..V.  NOISE: the first column, whose dot products read
+// features 1..9 with noise added (bmfr.cl:625-627).
+template <bool HALF, bool NOISE>
+__device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const NoiseTable& nt, NoiseConst nc,
+                                          FitterSmem& sm) {
+    const int V = kBuffers - 1 - col;
+    const float2 c01 = t.get2(0, 0), c23 = t.get2(0, 1);
+    const float c[4] = {c01.x, c01.y, c23.x, c23.y};
+    // Norm of rows >= col+1 (bmfr.cl:553-569); only row id (q = 0) can be above.
+    float nv[1];
+    {
+        float s = 0.0f;
+        if (id >= col + 1) s = s + c[0] * c[0];
+        s = s + c[1] * c[1];
+        s = s + c[2] * c[2];
+        s = s + c[3] * c[3];
+        nv[0] = s;
+    }
+    if (id == col) sm.ucl = c[0];
+    block_reduce<1, 0, 0>(nv, 1, 1, sm);
+    const float norm2 = sm.out[0];
+    const float ucl = sm.ucl;
+    // Work-item col's step (bmfr.cl:580-588), evaluated by every thread.
+    const float vl = sqrtf(norm2 + ucl * ucl);
+    const float ucl_new = ucl - vl;
+    const float uls = norm2 + ucl_new * ucl_new;
+    if (id < col) sm.Rm[col][id] = c[0];
+    if (id == col) sm.Rm[col][col] = vl;
+    float u[4] = {c[0], c[1], c[2], c[3]};
+    if (id == col) u[0] = ucl_new;
+    const bool row0 = id >= col;
+
+    // Dot products with the later columns (bmfr.cl:606-638).
+    float d[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        d[i] = 0.0f;
+        if (i < V) {
+            const float2 a01 = t.get2(i + 1, 0), a23 = t.get2(i + 1, 1);
+            float a[4] = {a01.x, a01.y, a23.x, a23.y};
+            if (NOISE && i + 1 < kFeatures) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], nt.r[i][q][threadIdx.x], nc);
+            }
+            float s = 0.0f;
+            if (row0) s = s + a[0] * u[0];
+            s = s + a[1] * u[1];
+            s = s + a[2] * u[2];
+            s = s + a[3] * u[3];
+            d[i] = s;
+        }
+    }
+    block_reduce<12, 0, 0>(d, V, V, sm);
+
+    // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
+    const float y = __frcp_rn(uls);
+    const bool fast = uls >= 0x1p-60f && uls <= 0x1p60f;
+    const float u2[4] = {2.0f * u[0], 2.0f * u[1], 2.0f * u[2], 2.0f * u[3]};
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        if (i < V) {
+            const float dot = sm.out[i];
+            const float2 a01 = t.get2(i + 1, 0), a23 = t.get2(i + 1, 1);
+            float a[4] = {a01.x, a01.y, a23.x, a23.y};
+            if (NOISE && i + 1 < kFeatures) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], nt.r[i][q][threadIdx.x], nc);
+            }
+            float n0 = a[0] - div_by(u2[0] * dot, uls, y, fast);
+            if (!row0) n0 = a[0];
+            const float n1 = a[1] - div_by(u2[1] * dot, uls, y, fast);
+            const float n2 = a[2] - div_by(u2[2] * dot, uls, y, fast);
+            const float n3 = a[3] - div_by(u2[3] * dot, uls, y, fast);
+            t.set2(i + 1, 0, n0, n1);
+            t.set2(i + 1, 1, n2, n3);
+        }
+    }
+    t.shift();
+}
+
 // Fits one block held in t (the values as loaded from tmp_data) and writes
-// its 30 weights and 12 min/max values.
-template <bool ROUND>
-__device__ __forceinline__ void fit_block(float (&t)[kBuffers][4], int frame, NoiseConst nc, FitterSmem& sm,
+// its 30 weights and 12 min/max values.  Ends with a barrier.
+template <bool HALF>
+__device__ __forceinline__ void fit_block(Tile<HALF>& t, const NoiseTable& nt, NoiseConst nc, FitterSmem& sm,
                                           float* __restrict__ weights_out, float* __restrict__ mm_out) {
     const int id = work_item_id();
     // Min/max scaling of features 4..9 (bmfr.cl:511-542).
     float mm[12];
 #pragma unroll
     for (int f = 0; f < kScaled; ++f) {
+        const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
+        const float a[4] = {a01.x, a01.y, a23.x, a23.y};
         float mx = -INFINITY, mn = INFINITY;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            mx = fmax_cl(t[kNotScaled + f][q], mx);
-            mn = fmin_cl(t[kNotScaled + f][q], mn);
+            mx = fmax_cl(a[q], mx);
+            mn = fmin_cl(a[q], mn);
         }
         mm[f] = mx;
         mm[kScaled + f] = mn;
     }
-    block_reduce<12, kScaled, 2, 1>(mm, sm);
+    block_reduce<12, 2, 1>(mm, 12, kScaled, sm);
     if (threadIdx.x < 2 * kScaled) {
         const int f = threadIdx.x >> 1;
         mm_out[threadIdx.x] = (threadIdx.x & 1) ? sm.out[f] : sm.out[kScaled + f];
@@ -207,34 +304,51 @@ __device__ __forceinline__ void fit_block(float (&t)[kBuffers][4], int frame, No
 #pragma unroll
     for (int f = 0; f < kScaled; ++f) {
         const float bmax = sm.out[f], bmin = sm.out[kScaled + f];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) t[kNotScaled + f][q] = stq<ROUND>(scale(t[kNotScaled + f][q], bmin, bmax));
+        const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
+        t.set2(kNotScaled + f, 0, scale(a01.x, bmin, bmax), scale(a01.y, bmin, bmax));
+        t.set2(kNotScaled + f, 1, scale(a23.x, bmin, bmax), scale(a23.y, bmin, bmax));
     }
 
-    QrColumn<0, ROUND>::run(t, id, frame, nc, sm);
+    qr_column<HALF, true>(t, 0, id, nt, nc, sm);
+#pragma unroll 1
+    for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, nt, nc, sm);
 
-    // R of the colour columns, rows 0..9 (bmfr.cl:596-600 for col >= 10).
+    // After ten shifts the colour columns are tile columns 0..2: rows 0..9
+    // form R's right-hand side (bmfr.cl:596-600 for col >= 10).
     if (id < kFeatures) {
-        sm.rhs[id][0] = t[kFeatures][0];
-        sm.rhs[id][1] = t[kFeatures + 1][0];
-        sm.rhs[id][2] = t[kFeatures + 2][0];
+        sm.rhs[id][0] = t.get2(0, 0).x;
+        sm.rhs[id][1] = t.get2(1, 0).x;
+        sm.rhs[id][2] = t.get2(2, 0).x;
     }
     __syncthreads();
-    // Back substitution, one thread per colour channel (bmfr.cl:659-699).
-    if (threadIdx.x < 3) {
-        const int c = threadIdx.x;
-        float(*R)[kREdge] = sm.Rb[c];
-        for (int x = 0; x < kFeatures; ++x)
-            for (int y = 0; y <= x; ++y) R[x][y] = sm.Rm[x][y];
-        for (int y = 0; y < kFeatures; ++y) R[kFeatures][y] = sm.rhs[y][c];
+    // Back substitution (bmfr.cl:659-699): warp c solves colour channel c,
+    // lane x owning column x of R.
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 3) {
+        const int c = warp;
+        float(*R)[12] = sm.Rb[c];
+        if (lane < kFeatures)
+            for (int y = 0; y <= lane; ++y) R[lane][y] = sm.Rm[lane][y];
+        if (lane == kFeatures)
+            for (int y = 0; y < kFeatures; ++y) R[kFeatures][y] = sm.rhs[y][c];
+        __syncwarp();
         for (int i = kREdge - 2; i >= 0; --i) {
             const float dv = R[i][i];
-            for (int x = i; x < kREdge; ++x) R[x][i] = R[x][i] / dv;
-            for (int j = i + 1; j < kREdge - 1; ++j) R[kREdge - 1][i] = R[kREdge - 1][i] - R[j][i];
-            for (int y = 0; y <= i; ++y) R[i][y] = R[i][y] * R[kREdge - 1][i];
+            __syncwarp();
+            if (lane >= i && lane < kREdge) R[lane][i] = R[lane][i] / dv;
+            __syncwarp();
+            if (lane == kREdge - 1) {
+                float v = R[kREdge - 1][i];
+                for (int jj = i + 1; jj < kREdge - 1; ++jj) v = v - R[jj][i];
+                R[kREdge - 1][i] = v;
+            }
+            __syncwarp();
+            if (lane <= i) R[i][lane] = R[i][lane] * R[kREdge - 1][i];
+            __syncwarp();
         }
-        for (int k = 0; k < kFeatures; ++k) weights_out[3 * k + c] = R[kREdge - 1][k];
+        if (lane < kFeatures) weights_out[3 * lane + c] = R[kREdge - 1][lane];
     }
+    __syncthreads();
 }
 
 }  // namespace bmfr

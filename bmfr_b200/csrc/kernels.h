@@ -14,8 +14,9 @@ cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float
                                     const float* prev_noisy, const uint8_t* prev_spp, uint8_t* cur_spp,
                                     void* tmp, cudaStream_t s);
 
+// status: device word that receives a nonzero code if a bounded wait ran out.
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                          bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s);
+                          bool fp32_qr, float* weights, float* mins_maxs, int* status, cudaStream_t s);
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,
                                 float* out, const float* cur_n, const float* cur_p, cudaStream_t s);

@@ -238,6 +238,23 @@ typedef struct bmfr_plan_buffers {
 } bmfr_plan_buffers;
 int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
 
+/* Per-stage timing of the plan pipeline, in place of the reference's
+ * per-kernel OpenCL event profiling (bmfr.cpp:386-412, 488-517).  While
+ * enabled, every denoise call records CUDA events between its stages.
+ * bmfr_plan_stage_times waits for the last frame and returns milliseconds of
+ * [accumulate_noisy_data, fitter, weighted_sum, accumulate_filtered_data,
+ * taa]; in the fused pipeline weighted_sum and accumulate_filtered_data are
+ * one kernel, reported at index 2 with index 3 = 0. */
+#define BMFR_STAGE_COUNT 5
+int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable);
+int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);
+
+/* Waits for `stream` and reports whether a kernel of this plan gave up a
+ * bounded wait (BMFR_E_TIMEOUT; the device status is then cleared).  The
+ * fitter waits on its bulk copies with a time limit instead of spinning
+ * without end. */
+int bmfr_plan_check_device(const bmfr_plan* plan, void* stream);
+
 /* Error text of the last failing call on this thread ("" if none). */
 const char* bmfr_last_error(void);
 const char* bmfr_status_string(int status);
