@@ -50,6 +50,7 @@ struct bmfr_plan {
     void* result[2] = {nullptr, nullptr};       // TAA history
     float* result_f32 = nullptr;                // fp32 output when histories are binary16
     int* dev_status = nullptr;                  // device error word (bounded waits)
+    float* noise_table = nullptr;               // the frame's fitter noise (scratch)
     const float* last_result = nullptr;         // float32 output of the last frame
     bool profiling = false;
     bool profiled_frame = false;
@@ -200,7 +201,7 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
          alloc(px * 12, &plan->filtered) && alloc(px * 8, &plan->prev_pix) && alloc(px, &plan->accept) &&
          alloc(px * 12, &plan->tone_mapped);
     if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32);
-    if (ok) ok = alloc(sizeof(int), &plan->dev_status);
+    if (ok) ok = alloc(sizeof(int), &plan->dev_status) && alloc(bmfr::kNoiseTableBytes, &plan->noise_table);
     if (!ok) {
         free_plan(plan);
         return fail(BMFR_E_NOMEM, "device allocation for the plan failed");
@@ -275,7 +276,7 @@ int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const v
     if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter: negative frame number");
     cudaError_t e = bmfr::launch_fitter(plan->g, frame_number, bmfr::make_noise_const(plan->p.noise_amount),
                                         tmp_data, plan->p.use_half_precision_in_tmp_data != 0,
-                                        plan->p.fp32_qr != 0, weights, mins_maxs, plan->dev_status,
+                                        plan->p.fp32_qr != 0, weights, mins_maxs, nullptr, plan->dev_status,
                                         (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
 }
@@ -369,13 +370,16 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         if (prof) cudaEventRecord(plan->events[i], s);
     };
     mark(0);
-    cudaError_t e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
+    cudaError_t e = bmfr::launch_noise_table(f, plan->noise_table, s);
+    if (e == cudaSuccess)
+        e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
                                                   noisy, plan->noisy_acc[cur], plan->noisy_acc[prv],
                                                   plan->spp[prv], plan->spp[cur], plan->tmp, s);
     mark(1);
     if (e == cudaSuccess)
         e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
-                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->dev_status, s);
+                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->noise_table,
+                                plan->dev_status, s);
     mark(2);
     bool split = false;
     if (e == cudaSuccess) {

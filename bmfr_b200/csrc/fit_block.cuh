@@ -29,8 +29,8 @@
 // same for the whole block.  Its correctly rounded reciprocal is formed once
 // and every quotient is taken with Markstein's correction step
 // (q = a*y; r = fma(-q, b, a); q' = fma(r, y, q)), which returns the
-// correctly rounded a/b for normal operands within 2^+-60; other operands
-// take a true division.
+// correctly rounded a/b while numerator, divisor and quotient stay normal;
+// operands outside the ranges that guarantee this take a true division.
 //
 // The colour columns' own reflections (columns 10..12, bmfr.cl:549 with
 // col_limited = 10) only change rows >= 10, which neither the back
@@ -107,14 +107,16 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
         }
     }
     // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right.
-    const int base = lane & ~7;
-    float r = __shfl_sync(kFull, s2, base);
+    if (warp < n) {   // warp-uniform: warps without a value skip
+        const int base = lane & ~7;
+        float r = __shfl_sync(kFull, s2, base);
 #pragma unroll
-    for (int m = 1; m < 8; ++m) {
-        const float x = __shfl_sync(kFull, s2, base + m);
-        r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
+        for (int m = 1; m < 8; ++m) {
+            const float x = __shfl_sync(kFull, s2, base + m);
+            r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
+        }
+        if (vi < n && j == 0) sm.out[vi] = r;
     }
-    if (vi < n && j == 0) sm.out[vi] = r;
     __syncthreads();
 }
 
@@ -168,38 +170,47 @@ __device__ __forceinline__ float add_noise_r(float value, float r, NoiseConst c)
 // at every call site.
 __device__ __noinline__ float div_slow(float a, float b) { return a / b; }
 
-// a / b correctly rounded, given y = RN(1/b) and fast = b within 2^+-60.
-__device__ __forceinline__ float div_by(float a, float b, float y, bool fast) {
-    const float q = a * y;
-    const float r = __fmaf_rn(-q, b, a);
-    const float q1 = __fmaf_rn(r, y, q);
-    const float aa = fabsf(a);
-    if (fast && aa >= 0x1p-60f && aa <= 0x1p60f) return q1;
-    if (a == 0.0f && fast) return a;   // +-0 / b, b > 0
-    return div_slow(a, b);
+// scale() (bmfr.cl:200-205) with the quotient taken by Markstein's
+// correction when numerator and divisor keep it normal.
+__device__ __forceinline__ float scale_by(float v, float mn, float mx) {
+    const float d = mx - mn;
+    const float num = v - mn;
+    if (!(fabsf(d) > 1.0f)) return num;
+    const float an = fabsf(num);
+    if (d <= 0x1p60f && (an == 0.0f || (an >= 0x1p-64f && an <= 0x1p60f))) {
+        const float y = __frcp_rn(d);
+        const float q0 = num * y;
+        const float r = __fmaf_rn(-q0, d, num);
+        return -__fmaf_rn(-r, y, -q0);
+    }
+    return div_slow(num, d);
 }
 
-// Shared-memory table of the fitter's feature noise r = random(i) - 0.5 for
-// features 1..9 and this thread's four rows; the same for every block of a
-// frame (bmfr.cl:179-181 does not involve the block index).
-struct NoiseTable {
-    float r[kFeatures - 1][4][kLocal];
-};
+// Table of the fitter's feature noise r = random(i) - 0.5 (bmfr.cl:179-181)
+// for features 1..9, laid out [feature-1][row group q][thread] so that each
+// thread reads its own four rows coalesced.  It does not involve the block
+// index, so one table serves every block of a frame; it lives in shared
+// memory (standalone fitter) or global memory (frame pipeline).
+constexpr int kNoiseTableFloats = (kFeatures - 1) * 4 * kLocal;
 
-__device__ __forceinline__ void fill_noise_table(NoiseTable& nt, int frame) {
-    const int id = work_item_id();
-#pragma unroll
-    for (int fb = 1; fb < kFeatures; ++fb)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) nt.r[fb - 1][q][threadIdx.x] = hash_random(noise_index(id, q, fb, frame)) - 0.5f;
+__device__ __forceinline__ float noise_table_value(int entry, int frame) {
+    const int tx = entry % kLocal, fq = entry / kLocal;   // fq = (fb-1)*4 + q
+    const int fb = fq / 4 + 1, q = fq % 4;
+    const int warp = tx >> 5, lane = tx & 31;
+    const int id = 8 * warp + (lane & 7) + 64 * (lane >> 3);
+    return hash_random(noise_index(id, q, fb, frame)) - 0.5f;
+}
+
+__device__ __forceinline__ void fill_noise_table(float* table, int frame) {
+    for (int e = threadIdx.x; e < kNoiseTableFloats; e += kLocal) table[e] = noise_table_value(e, frame);
 }
 
 // One Householder column (bmfr.cl:549-655) on tile column 0; later columns
 // are tile columns 1..V.  NOISE: the first column, whose dot products read
 // features 1..9 with noise added (bmfr.cl:625-627).
 template <bool HALF, bool NOISE>
-__device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const NoiseTable& nt, NoiseConst nc,
-                                          FitterSmem& sm) {
+__device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const float* __restrict__ noise,
+                                          NoiseConst nc, FitterSmem& sm) {
     const int V = kBuffers - 1 - col;
     const float2 c01 = t.get2(0, 0), c23 = t.get2(0, 1);
     const float c[4] = {c01.x, c01.y, c23.x, c23.y};
@@ -237,7 +248,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             float a[4] = {a01.x, a01.y, a23.x, a23.y};
             if (NOISE && i + 1 < kFeatures) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], nt.r[i][q][threadIdx.x], nc);
+                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], noise[(i * 4 + q) * kLocal + threadIdx.x], nc);
             }
             float s = 0.0f;
             if (row0) s = s + a[0] * u[0];
@@ -250,26 +261,48 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     block_reduce<12, 0, 0>(d, V, V, sm);
 
     // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
+    // Quotients take Markstein's correction when every operand is in range:
+    // |u| and |dot| within [2^-32, 2^30] (or zero) and |u|^2 within 2^+-60
+    // keep numerator and quotient normal.
     const float y = __frcp_rn(uls);
-    const bool fast = uls >= 0x1p-60f && uls <= 0x1p60f;
+    const bool fast_b = uls >= 0x1p-60f && uls <= 0x1p60f;
     const float u2[4] = {2.0f * u[0], 2.0f * u[1], 2.0f * u[2], 2.0f * u[3]};
+    bool fast_u = fast_b;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float a = fabsf(u2[q]);
+        fast_u = fast_u && (a == 0.0f || (a >= 0x1p-32f && a <= 0x1p30f));
+    }
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
         if (i < V) {
             const float dot = sm.out[i];
+            const float ad = fabsf(dot);
+            const bool fast = fast_u && (ad == 0.0f || (ad >= 0x1p-32f && ad <= 0x1p30f));
             const float2 a01 = t.get2(i + 1, 0), a23 = t.get2(i + 1, 1);
             float a[4] = {a01.x, a01.y, a23.x, a23.y};
             if (NOISE && i + 1 < kFeatures) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], nt.r[i][q][threadIdx.x], nc);
+                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], noise[(i * 4 + q) * kLocal + threadIdx.x], nc);
             }
-            float n0 = a[0] - div_by(u2[0] * dot, uls, y, fast);
-            if (!row0) n0 = a[0];
-            const float n1 = a[1] - div_by(u2[1] * dot, uls, y, fast);
-            const float n2 = a[2] - div_by(u2[2] * dot, uls, y, fast);
-            const float n3 = a[3] - div_by(u2[3] * dot, uls, y, fast);
-            t.set2(i + 1, 0, n0, n1);
-            t.set2(i + 1, 1, n2, n3);
+            float n[4];
+            if (fast) {
+                // a - RN(num / uls) as a + (-q1): the negated form keeps the
+                // sign of zero quotients exact without a select.
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float num = u2[q] * dot;
+                    const float q0 = num * y;
+                    const float r = __fmaf_rn(-q0, uls, num);
+                    n[q] = a[q] + __fmaf_rn(-r, y, -q0);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) n[q] = a[q] - div_slow(u2[q] * dot, uls);
+            }
+            if (!row0) n[0] = a[0];
+            t.set2(i + 1, 0, n[0], n[1]);
+            t.set2(i + 1, 1, n[2], n[3]);
         }
     }
     t.shift();
@@ -278,8 +311,9 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
 // Fits one block held in t (the values as loaded from tmp_data) and writes
 // its 30 weights and 12 min/max values.  Ends with a barrier.
 template <bool HALF>
-__device__ __forceinline__ void fit_block(Tile<HALF>& t, const NoiseTable& nt, NoiseConst nc, FitterSmem& sm,
-                                          float* __restrict__ weights_out, float* __restrict__ mm_out) {
+__device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict__ noise, NoiseConst nc,
+                                          FitterSmem& sm, float* __restrict__ weights_out,
+                                          float* __restrict__ mm_out) {
     const int id = work_item_id();
     // Min/max scaling of features 4..9 (bmfr.cl:511-542).
     float mm[12];
@@ -305,13 +339,13 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const NoiseTable& nt, N
     for (int f = 0; f < kScaled; ++f) {
         const float bmax = sm.out[f], bmin = sm.out[kScaled + f];
         const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
-        t.set2(kNotScaled + f, 0, scale(a01.x, bmin, bmax), scale(a01.y, bmin, bmax));
-        t.set2(kNotScaled + f, 1, scale(a23.x, bmin, bmax), scale(a23.y, bmin, bmax));
+        t.set2(kNotScaled + f, 0, scale_by(a01.x, bmin, bmax), scale_by(a01.y, bmin, bmax));
+        t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
     }
 
-    qr_column<HALF, true>(t, 0, id, nt, nc, sm);
+    qr_column<HALF, true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1
-    for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, nt, nc, sm);
+    for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);
 
     // After ten shifts the colour columns are tile columns 0..2: rows 0..9
     // form R's right-hand side (bmfr.cl:596-600 for col >= 10).

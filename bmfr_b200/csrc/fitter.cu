@@ -1,31 +1,38 @@
 // fitter.cu — standalone fitter kernel (opencl/bmfr.cl:490-700).
 //
-// Persistent CTAs of 256 threads, as many as fit on the SMs (three per SM for
-// the binary16 block).  Each CTA forms its frame's feature-noise table once,
-// then walks blocks b = blockIdx.x, + gridDim.x, ...: the block's 13 x 1024
-// tmp_data values arrive by one bulk TMA copy (contiguous 26 KB, no tensor
-// map needed) into shared memory, move to registers, and the copy of the
-// CTA's next block is issued at once so that it overlaps the fit.
+// Persistent CTAs of 256 threads, as many as fit on the SMs.  Each CTA walks
+// blocks b = blockIdx.x, + gridDim.x, ...: the block's 13 x 1024 tmp_data
+// values arrive by one bulk TMA copy (contiguous 26 KB, no tensor map
+// needed) into shared memory, move to registers, and the copy of the CTA's
+// next block is issued at once so that it overlaps the fit.
+//
+// The feature-noise table of the frame is either formed by each CTA in its
+// shared memory (the drop-in entry point: no scratch memory, so calls on
+// different streams never share state) or read from a table that an earlier
+// kernel of the frame pipeline wrote to global memory (smaller CTAs, more of
+// them per SM).
+#include <type_traits>
+
 #include "fit_block.cuh"
 #include "kernels.h"
 #include "tma.cuh"
 
 namespace bmfr {
 
-template <bool HALF_TMP>
+template <bool HALF_TMP, bool NOISE_GLOBAL>
 struct FitterShared {
     using TmpT = typename std::conditional<HALF_TMP, __half, float>::type;
-    NoiseTable nt;
-    FitterSmem sm;
     alignas(128) TmpT tile[kBuffers * kBlockPixels];
+    FitterSmem sm;
     alignas(8) uint64_t bar;
+    float noise[NOISE_GLOBAL ? 1 : kNoiseTableFloats];
 };
 
-template <bool HALF_TMP, bool ROUND>
-__global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
+template <bool HALF_TMP, bool ROUND, bool NOISE_GLOBAL>
+__global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? (NOISE_GLOBAL ? 4 : 3) : 2)
     k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, float* __restrict__ weights,
-             float* __restrict__ mins_maxs, int* __restrict__ status) {
-    using Shared = FitterShared<HALF_TMP>;
+             float* __restrict__ mins_maxs, const float* __restrict__ noise_g, int* __restrict__ status) {
+    using Shared = FitterShared<HALF_TMP, NOISE_GLOBAL>;
     using TmpT = typename Shared::TmpT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Shared& S = *reinterpret_cast<Shared*>(smem_raw);
@@ -43,7 +50,8 @@ __global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
             bulk_copy_g2s(S.tile, src + (size_t)b * kTileBytes, kTileBytes, &S.bar);
         }
     }
-    fill_noise_table(S.nt, frame);
+    if (!NOISE_GLOBAL) fill_noise_table(S.noise, frame);
+    const float* noise = NOISE_GLOBAL ? noise_g : S.noise;
     __syncthreads();
 
     uint32_t phase = 0;
@@ -78,21 +86,33 @@ __global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
             mbar_arrive_expect_tx(&S.bar, kTileBytes);
             bulk_copy_g2s(S.tile, src + (size_t)next * kTileBytes, kTileBytes, &S.bar);
         }
-        fit_block<ROUND>(t, S.nt, nc, S.sm, weights + (size_t)b * kFeatures * 3, mins_maxs + (size_t)b * kScaled * 2);
+        fit_block<ROUND>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3, mins_maxs + (size_t)b * kScaled * 2);
     }
 }
 
-template <bool HALF_TMP, bool ROUND>
+// The frame's noise table in global memory (kNoiseTableFloats floats).
+__global__ void __launch_bounds__(256) k_noise_table(int frame, float* __restrict__ table) {
+    const int e = blockIdx.x * kLocal + threadIdx.x;
+    if (e < kNoiseTableFloats) table[e] = noise_table_value(e, frame);
+}
+
+cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s) {
+    k_noise_table<<<kNoiseTableFloats / kLocal, kLocal, 0, s>>>(frame, table);
+    return cudaGetLastError();
+}
+
+template <bool HALF_TMP, bool ROUND, bool NOISE_GLOBAL>
 static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const void* tmp, float* weights,
-                                   float* mins_maxs, int* status, cudaStream_t s) {
-    auto kern = k_fitter<HALF_TMP, ROUND>;
-    const int smem = (int)sizeof(FitterShared<HALF_TMP>);
+                                   float* mins_maxs, const float* noise, int* status, cudaStream_t s) {
+    auto kern = k_fitter<HALF_TMP, ROUND, NOISE_GLOBAL>;
+    const int smem = (int)sizeof(FitterShared<HALF_TMP, NOISE_GLOBAL>);
     static int grid_cap[64] = {0};   // per device
     int dev = 0;
-    cudaGetDevice(&dev);
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (grid_cap[dev] == 0) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         int per_sm = 0, sms = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLocal, smem);
@@ -103,15 +123,25 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
     }
     const int grid = nblocks < grid_cap[dev] ? nblocks : grid_cap[dev];
     if (grid <= 0) return cudaSuccess;
-    kern<<<grid, kLocal, smem, s>>>(nblocks, frame, nc, tmp, weights, mins_maxs, status);
+    kern<<<grid, kLocal, smem, s>>>(nblocks, frame, nc, tmp, weights, mins_maxs, noise, status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                          bool fp32_qr, float* weights, float* mins_maxs, int* status, cudaStream_t s) {
-    if (half_tmp && !fp32_qr) return launch_fitter_t<true, true>(g.blocks, frame, nc, tmp, weights, mins_maxs, status, s);
-    if (half_tmp) return launch_fitter_t<true, false>(g.blocks, frame, nc, tmp, weights, mins_maxs, status, s);
-    return launch_fitter_t<false, false>(g.blocks, frame, nc, tmp, weights, mins_maxs, status, s);
+                          bool fp32_qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
+                          cudaStream_t s) {
+    const int n = g.blocks;
+    if (noise_table) {
+        if (half_tmp && !fp32_qr)
+            return launch_fitter_t<true, true, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
+        if (half_tmp)
+            return launch_fitter_t<true, false, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
+        return launch_fitter_t<false, false, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
+    }
+    if (half_tmp && !fp32_qr)
+        return launch_fitter_t<true, true, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
+    if (half_tmp) return launch_fitter_t<true, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
+    return launch_fitter_t<false, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
 }
 
 }  // namespace bmfr

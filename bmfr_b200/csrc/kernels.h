@@ -15,8 +15,13 @@ cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float
                                     void* tmp, cudaStream_t s);
 
 // status: device word that receives a nonzero code if a bounded wait ran out.
+// noise_table: the frame's table from launch_noise_table, or null to have
+// every CTA form it in shared memory.
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                          bool fp32_qr, float* weights, float* mins_maxs, int* status, cudaStream_t s);
+                          bool fp32_qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
+                          cudaStream_t s);
+cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s);
+constexpr size_t kNoiseTableBytes = 9 * 4 * 256 * sizeof(float);
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,
                                 float* out, const float* cur_n, const float* cur_p, cudaStream_t s);
