@@ -64,6 +64,11 @@ def stage_bytes(w, h):
         "accumulate_filtered_data": 70 * P,
         "weighted_sum+accumulate_filtered_data": 82 * P,
         "taa": 44 * P,
+        "noise_table": 9 * 4 * 256 * 4,
+        # accumulate (95 B/px + 26 B read per margin pixel from the inputs, no
+        # tmp_data) + weighted sum and filtered accumulation (82 B/px less the
+        # 24 B/px of N, P re-read from L2) -> counted once per byte of HBM.
+        "block_kernel": 95 * P + 24 * (Pm - P) + 168 * B + 58 * P,
     }
 
 
@@ -258,22 +263,21 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         elapsed_ms = float(t.item())
     value = world * args.steps / (elapsed_ms / 1e3)
-    launches_per_frame = 4   # accumulate, fitter, weighted_sum+accumulate_filtered, taa
+    # noise table, block kernel, taa (fused); noise table, accumulate, fitter,
+    # weighted_sum, accumulate_filtered, taa (staged)
+    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 6
 
     # ---- per-stage profile (same workload, events between stages) ------------
     plan.enable_profiling(True)
-    stage_ms = {k: [] for k in B.Plan.STAGES}
+    stage_ms = {}
     base = args.warmup + args.steps
     nprof = min(args.steps, 60)
     for i in range(base, base + nprof):
         step_resident(i)
         for k, v in plan.stage_times().items():
-            stage_ms[k].append(v)
+            stage_ms.setdefault(k, []).append(v)
     plan.enable_profiling(False)
-    stages = {k: float(np.mean(v)) for k, v in stage_ms.items()}
-    if pipeline == B.PIPELINE_FUSED:
-        stages["weighted_sum+accumulate_filtered_data"] = stages.pop("weighted_sum")
-        stages.pop("accumulate_filtered_data")
+    stages = {k: float(np.mean(v)) for k, v in stage_ms.items() if v}
     sb = stage_bytes(WIDTH, HEIGHT)
     dominant = max(stages, key=stages.get)
     hbm_peak, peak_kind = peaks()

@@ -188,12 +188,15 @@ class Plan:
         check(lib.bmfr_plan_enable_profiling(self.handle, int(enable)), "bmfr_plan_enable_profiling")
 
     STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa")
+    FUSED_STAGES = ("noise_table", "block_kernel", None, None, "taa")
 
     def stage_times(self) -> dict:
-        """Milliseconds per stage of the last profiled frame."""
+        """Milliseconds per kernel of the last profiled frame (the staged
+        pipeline's five stages, or the fused pipeline's three kernels)."""
         ms = (C.c_float * 5)()
         check(lib.bmfr_plan_stage_times(self.handle, ms), "bmfr_plan_stage_times")
-        return dict(zip(self.STAGES, map(float, ms)))
+        names = self.FUSED_STAGES if self.params.pipeline == PIPELINE_FUSED else self.STAGES
+        return {n: float(v) for n, v in zip(names, ms) if n is not None}
 
     def buffers(self) -> PlanBuffers:
         b = PlanBuffers()

@@ -37,7 +37,7 @@ struct bmfr_plan {
     float* positions[2] = {nullptr, nullptr};
     float* albedo = nullptr;
     float* noisy_in = nullptr;        // this frame's 1-spp colour
-    float* noisy_acc[2] = {nullptr, nullptr};   // accumulated noisy history
+    void* noisy_acc[2] = {nullptr, nullptr};    // accumulated noisy history
     uint8_t* spp[2] = {nullptr, nullptr};
     void* tmp = nullptr;
     float* weights = nullptr;
@@ -160,6 +160,8 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
     if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
         return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    if (params->half_history && params->pipeline != BMFR_PIPELINE_FUSED)
+        return fail(BMFR_E_UNSUPPORTED, "binary16 histories need the fused pipeline");
     if (params->pipeline != BMFR_PIPELINE_STAGED && params->pipeline != BMFR_PIPELINE_FUSED)
         return fail(BMFR_E_INVALID, "unknown pipeline");
     if (!(params->blend_alpha > 0.f) || !(params->second_blend_alpha > 0.f))
@@ -190,7 +192,7 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
     bool ok = true;
     for (int i = 0; i < 2 && ok; ++i) {
         ok = ok && alloc(px * 12, &plan->normals[i]) && alloc(px * 12, &plan->positions[i]) &&
-             alloc(px * 12, &plan->noisy_acc[i]) && alloc(px, &plan->spp[i]) &&
+             alloc(pixel3_bytes(plan, half_hist), &plan->noisy_acc[i]) && alloc(px, &plan->spp[i]) &&
              alloc(pixel3_bytes(plan, half_hist), &plan->acc_filt[i]) &&
              alloc(pixel3_bytes(plan, half_hist), &plan->result[i]);
     }
@@ -371,33 +373,51 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     };
     mark(0);
     cudaError_t e = bmfr::launch_noise_table(f, plan->noise_table, s);
-    if (e == cudaSuccess)
-        e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
-                                                  noisy, plan->noisy_acc[cur], plan->noisy_acc[prv],
-                                                  plan->spp[prv], plan->spp[cur], plan->tmp, s);
-    mark(1);
-    if (e == cudaSuccess)
-        e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
-                                plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->noise_table,
-                                plan->dev_status, s);
-    mark(2);
     bool split = false;
-    if (e == cudaSuccess) {
-        if (plan->p.pipeline == BMFR_PIPELINE_STAGED && !half_hist) {
-            split = true;
+    if (plan->p.pipeline == BMFR_PIPELINE_FUSED) {
+        mark(1);
+        bmfr::FusedBuffers fb;
+        fb.cur_n = cur_n;
+        fb.prev_n = prev_n;
+        fb.cur_p = cur_p;
+        fb.prev_p = prev_p;
+        fb.noisy_in = noisy;
+        fb.albedo = albedo;
+        fb.noisy_acc_cur = plan->noisy_acc[cur];
+        fb.noisy_acc_prev = plan->noisy_acc[prv];
+        fb.prev_spp = plan->spp[prv];
+        fb.cur_spp = plan->spp[cur];
+        fb.prev_pix = plan->prev_pix;
+        fb.accept = plan->accept;
+        fb.tone_mapped = plan->tone_mapped;
+        fb.acc_prev = plan->acc_filt[prv];
+        fb.acc_cur = plan->acc_filt[cur];
+        fb.weights = plan->weights;
+        fb.mins_maxs = plan->mins_maxs;
+        fb.noise = plan->noise_table;
+        if (e == cudaSuccess)
+            e = bmfr::launch_fused_block(g, a, bmfr::make_noise_const(plan->p.noise_amount),
+                                         plan->p.second_blend_alpha, plan->p.fp32_qr != 0, half_hist, fb, s);
+        mark(2);
+    } else {
+        if (e == cudaSuccess)
+            e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
+                                              noisy, (float*)plan->noisy_acc[cur], (const float*)plan->noisy_acc[prv],
+                                              plan->spp[prv], plan->spp[cur], plan->tmp, s);
+        mark(1);
+        if (e == cudaSuccess)
+            e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
+                                    plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->noise_table,
+                                    plan->dev_status, s);
+        mark(2);
+        split = true;
+        if (e == cudaSuccess)
             e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
-            mark(3);
-            if (e == cudaSuccess)
-                e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered,
-                                                     plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
-                                                     plan->spp[cur], (const float*)plan->acc_filt[prv],
-                                                     (float*)plan->acc_filt[cur], s);
-        } else {
-            e = bmfr::launch_weighted_sum_accumulate(
-                g, f, plan->p.second_blend_alpha, plan->weights, plan->mins_maxs, cur_n, cur_p,
-                plan->p.pipeline == BMFR_PIPELINE_STAGED ? plan->filtered : nullptr, plan->prev_pix, plan->accept,
-                albedo, plan->tone_mapped, plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur], half_hist, s);
-        }
+        mark(3);
+        if (e == cudaSuccess)
+            e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered, plan->prev_pix,
+                                                 plan->accept, albedo, plan->tone_mapped, plan->spp[cur],
+                                                 (const float*)plan->acc_filt[prv], (float*)plan->acc_filt[cur], s);
     }
     if (!split) mark(3);
     mark(4);

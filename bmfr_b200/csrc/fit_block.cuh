@@ -168,7 +168,7 @@ __device__ __forceinline__ float add_noise_r(float value, float r, NoiseConst c)
 
 // True division, kept out of line so that the rare slow case costs no code
 // at every call site.
-__device__ __noinline__ float div_slow(float a, float b) { return a / b; }
+static __device__ __noinline__ float div_slow(float a, float b) { return a / b; }
 
 // scale() (bmfr.cl:200-205) with the quotient taken by Markstein's
 // correction when numerator and divisor keep it normal.

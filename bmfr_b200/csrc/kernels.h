@@ -42,6 +42,27 @@ cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const floa
                        const float* new_frame, void* result, const void* prev_frame, float* result_f32,
                        bool half_history, cudaStream_t s);
 
+// Buffers of the fused block kernel (accumulate + fit + weighted sum +
+// filtered accumulation).  The four colour histories are float or binary16
+// per the launch's half_history.
+struct FusedBuffers {
+    const float *cur_n, *prev_n, *cur_p, *prev_p, *noisy_in, *albedo;
+    void* noisy_acc_cur;
+    const void* noisy_acc_prev;
+    const uint8_t* prev_spp;
+    uint8_t* cur_spp;
+    float2* prev_pix;
+    uint8_t* accept;
+    float* tone_mapped;
+    const void* acc_prev;
+    void* acc_cur;
+    float *weights, *mins_maxs;
+    const float* noise;   // the frame's noise table (launch_noise_table)
+};
+
+cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
+                               bool fp32_qr, bool half_history, const FusedBuffers& fb, cudaStream_t s);
+
 // NOISE_AMOUNT * 2 split into hi + lo floats.
 inline NoiseConst make_noise_const(double noise_amount) {
     const double c = noise_amount * 2.0;

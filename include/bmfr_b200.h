@@ -242,9 +242,10 @@ int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
  * per-kernel OpenCL event profiling (bmfr.cpp:386-412, 488-517).  While
  * enabled, every denoise call records CUDA events between its stages.
  * bmfr_plan_stage_times waits for the last frame and returns milliseconds of
- * [accumulate_noisy_data, fitter, weighted_sum, accumulate_filtered_data,
- * taa]; in the fused pipeline weighted_sum and accumulate_filtered_data are
- * one kernel, reported at index 2 with index 3 = 0. */
+ * the staged pipeline's [accumulate_noisy_data (with the frame's fitter
+ * noise table), fitter, weighted_sum, accumulate_filtered_data, taa].  The
+ * fused pipeline reports [noise table, block kernel (accumulate, fitter,
+ * weighted sum and filtered accumulation), 0, 0, taa]. */
 #define BMFR_STAGE_COUNT 5
 int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable);
 int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);

@@ -11,6 +11,32 @@ from test_parity_stages import assert_close
 pytestmark = pytest.mark.gpu
 
 
+def _cudart():
+    import ctypes
+    import glob
+    import os
+    import torch
+    cands = glob.glob(os.path.join(os.path.dirname(torch.__file__), "..", "nvidia", "cuda_runtime", "lib",
+                                   "libcudart.so*")) + ["/usr/local/cuda/lib64/libcudart.so"]
+    for c in cands:
+        try:
+            lib = ctypes.CDLL(c)
+            lib.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+            return lib
+        except OSError:
+            continue
+    raise RuntimeError("no CUDA runtime to read device buffers")
+
+
+def device_array(ptr, shape, dtype):
+    """Copies `shape` elements at device address `ptr` to a numpy array."""
+    import torch
+    torch.cuda.synchronize()
+    out = np.empty(shape, dtype=dtype)
+    assert _cudart().cudaMemcpy(out.ctypes.data, ptr, out.nbytes, 2) == 0
+    return out
+
+
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
 @pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
@@ -27,6 +53,19 @@ def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
         want = ref.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f),
                         sc.pixel_offset(f))
         assert_close(got, want, f"result frame {f}", rtol=1e-4)
+        # Intermediates of the frame: integer outputs and the fit bit-exact.
+        bufs = plan.buffers()
+        c = f & 1
+        np.testing.assert_array_equal(device_array(bufs.accept, (H, W), np.uint8), ref.accept)
+        np.testing.assert_array_equal(device_array(bufs.spp, (H, W), np.uint8), ref.spp[c])
+        np.testing.assert_array_equal(device_array(bufs.prev_frame_pixel, (H, W, 2), np.float32), ref.prev_pix)
+        np.testing.assert_array_equal(device_array(bufs.mins_maxs, ref.mins_maxs.shape, np.float32),
+                                      ref.mins_maxs)
+        gw = device_array(bufs.weights, ref.weights.shape, np.float32)
+        assert (gw == ref.weights).mean() > 0.99, f"weights frame {f}"
+        np.testing.assert_array_equal(device_array(bufs.accumulated_noisy, (H, W, 3), np.float32), ref.noisy[c])
+        assert_close(device_array(bufs.tone_mapped, (H, W, 3), np.float32), ref.tone_mapped, "tone mapped",
+                     rtol=1e-5)
     torch.cuda.synchronize()
     assert plan.frame_number == frames
     plan.close()
