@@ -149,6 +149,23 @@ int bmfr_block_offsets(int out_xy[32]) {
     return BMFR_OK;
 }
 
+namespace {
+
+// The checks of bmfr_plan_create, for the entry point that takes no plan.
+int validate(const bmfr_params* params, int width, int height) {
+    if (width < 32 || height < 32 || width > 16384 || height > 16384)
+        return fail(BMFR_E_INVALID, "image size must be within [32, 16384]");
+    const bmfr::Geometry g = bmfr::make_geometry(width, height);
+    // mirror() (bmfr.cl:209-216) must stay within one image size: the margin
+    // grid reaches WORKSET + 29 on the right/bottom and -32 on the left/top.
+    if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
+        return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
+    if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    return BMFR_OK;
+}
+
+}  // namespace
+
 int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan** out) {
     if (!params || !out) return fail(BMFR_E_INVALID, "params/plan pointer is NULL");
     *out = nullptr;
@@ -281,6 +298,21 @@ int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const v
                                         plan->p.fp32_qr != 0, weights, mins_maxs, nullptr, plan->dev_status,
                                         (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
+}
+
+int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height, float* weights, float* mins_maxs,
+                        const void* tmp_data, int frame_number, void* stream) {
+    if (!params) return fail(BMFR_E_INVALID, "fitter_noalloc: params is NULL");
+    if (int st = validate(params, width, height)) return st;
+    if (!weights || !mins_maxs || !tmp_data) return fail(BMFR_E_INVALID, "fitter_noalloc: NULL buffer");
+    if (reinterpret_cast<uintptr_t>(tmp_data) % 16 != 0)
+        return fail(BMFR_E_INVALID, "fitter_noalloc: tmp_data must be 16-byte aligned");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter_noalloc: negative frame number");
+    const bmfr::Geometry g = bmfr::make_geometry(width, height);
+    cudaError_t e = bmfr::launch_fitter_static(g, frame_number, bmfr::make_noise_const(params->noise_amount),
+                                               tmp_data, params->use_half_precision_in_tmp_data != 0,
+                                               params->fp32_qr != 0, weights, mins_maxs, (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter_noalloc launch");
 }
 
 int bmfr_weighted_sum(const bmfr_plan* plan, const float* weights, const float* mins_maxs, float* output,

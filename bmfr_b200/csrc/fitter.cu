@@ -11,6 +11,7 @@
 // different streams never share state) or read from a table that an earlier
 // kernel of the frame pipeline wrote to global memory (smaller CTAs, more of
 // them per SM).
+#include <mutex>
 #include <type_traits>
 
 #include "fit_block.cuh"
@@ -142,6 +143,53 @@ cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const voi
         return launch_fitter_t<true, true, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
     if (half_tmp) return launch_fitter_t<true, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
     return launch_fitter_t<false, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
+}
+
+// ---------------------------------------------------------------------------
+// Scratch in a static device array, for callers that cannot allocate.
+//
+// The fitter's scratch is the frame's noise table (kNoiseTableFloats floats)
+// plus the bounded-wait status word.  Both live here in one file-scope device
+// array, so launch_fitter_static needs no cudaMalloc.  The table does not
+// grow with the image: this fixed size serves every image size a plan
+// accepts.  In host code g_fitter_scratch only names the symbol; the device
+// address comes from cudaGetSymbolAddress, taken once per device with that
+// device current.
+constexpr size_t kStaticStatusOffset = kNoiseTableBytes;             // 36,864
+constexpr size_t kStaticScratchBytes = kStaticStatusOffset + 256;    // table + status word
+static __device__ __align__(256) unsigned char g_fitter_scratch[kStaticScratchBytes];
+
+static std::mutex g_scratch_mutex;
+static void* g_scratch_address[64] = {nullptr};
+
+static cudaError_t static_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_address[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_fitter_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_address[dev] = p;
+    }
+    *out = g_scratch_address[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
+                                 bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s) {
+    void* base = nullptr;
+    cudaError_t e = static_scratch_address(&base);
+    if (e != cudaSuccess) return e;
+    float* table = static_cast<float*>(base);
+    int* status = reinterpret_cast<int*>(static_cast<unsigned char*>(base) + kStaticStatusOffset);
+    e = cudaMemsetAsync(status, 0, sizeof(int), s);   // the array keeps the last call's contents
+    if (e != cudaSuccess) return e;
+    e = launch_noise_table(frame, table, s);
+    if (e != cudaSuccess) return e;
+    return launch_fitter(g, frame, nc, tmp, half_tmp, fp32_qr, weights, mins_maxs, table, status, s);
 }
 
 }  // namespace bmfr

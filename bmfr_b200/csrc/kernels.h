@@ -21,6 +21,9 @@ cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const voi
                           bool fp32_qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
                           cudaStream_t s);
 cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s);
+// The fitter with its scratch in a static device array (no allocation).
+cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
+                                 bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s);
 constexpr size_t kNoiseTableBytes = 9 * 4 * 256 * sizeof(float);
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,

@@ -150,6 +150,26 @@ int bmfr_accumulate_noisy_data(const bmfr_plan* plan,
 int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs,
                 const void* tmp_data, int frame_number, void* stream);
 
+/* bmfr_fitter without any device allocation; no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: renderers whose engine
+ * owns all device memory under a fixed budget, and per-frame code that cannot
+ * afford cudaMalloc's implicit device synchronisation.  It needs no plan
+ * (creating one allocates the history buffers): the sizes come from
+ * width/height and the options from params.  The fitter's scratch — the
+ * frame's noise table and a status word, 37,120 bytes — lives in a static
+ * device array of the library that every GPU loading the library holds until
+ * the process exits; its size does not grow with the image, so every size a
+ * plan accepts is served and larger sizes are rejected like plan creation
+ * rejects them.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  All calls share the array and each call
+ * rewrites it, so calls whose kernels overlap on the GPU (different streams,
+ * or one stream and another without ordering) race: order them.  Results
+ * equal bmfr_fitter's. */
+int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height,
+                        float* weights, float* mins_maxs, const void* tmp_data,
+                        int frame_number, void* stream);
+
 /* weighted_sum (bmfr.cl:703-758). current_noisy is unused, as in the
  * reference (debug only, bmfr.cl:709), and may be NULL. */
 int bmfr_weighted_sum(const bmfr_plan* plan, const float* weights,
