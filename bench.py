@@ -195,7 +195,7 @@ def main():
     ap.add_argument("--steps", type=int, default=240)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--pipeline", default="fused", choices=["fused", "staged"])
+    ap.add_argument("--pipeline", default="staged", choices=["fused", "staged"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=FRAMES, help="distinct scene frames held in HBM")
     args = ap.parse_args()

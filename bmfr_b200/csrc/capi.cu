@@ -137,7 +137,7 @@ int bmfr_params_default(bmfr_params* p) {
     p->cache_tmp_data = 1;             // bmfr.cpp:84
     p->fp32_qr = 0;
     p->half_history = 0;
-    p->pipeline = BMFR_PIPELINE_FUSED;
+    p->pipeline = BMFR_PIPELINE_STAGED;
     return BMFR_OK;
 }
 

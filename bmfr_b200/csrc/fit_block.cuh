@@ -48,7 +48,7 @@ struct FitterSmem {
     int status;            // nonzero: a bounded wait ran out
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
-    float Rb[3][11][12];   // per-channel copy used by the back substitution
+    float part2[12 * 8];   // second-stage sums, 8 per batched value
 };
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -70,19 +70,38 @@ __device__ __forceinline__ float rop(float a, float b) {
 template <int VMAX, int OP_A, int OP_B>
 __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int split, FitterSmem& sm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (OP_A == 0 && OP_B == 0) {
+        // Sums, two values per packed add (bmfr.cl:33).
 #pragma unroll
-    for (int i = 0; i < VMAX; ++i) {
-        if (i < n) {
-            const float a = v[i];
-            const float b = __shfl_down_sync(kFull, a, 8);
-            const float c = __shfl_down_sync(kFull, a, 16);
-            const float d = __shfl_down_sync(kFull, a, 24);
-            const int op = i < split ? OP_A : OP_B;
-            float s1;
-            if (op == 0) s1 = a + ((b + c) + d);                               // bmfr.cl:33
-            else if (op == 1) s1 = fmin_cl(fmin_cl(fmin_cl(a, b), c), d);    // bmfr.cl:52-53
-            else s1 = fmax_cl(fmax_cl(fmax_cl(a, b), c), d);                 // bmfr.cl:74-75
-            if (lane < 8) sm.part[i * 64 + 8 * warp + lane] = s1;
+        for (int i = 0; i < VMAX; i += 2) {
+            if (i < n) {
+                const float a0 = v[i], a1 = i + 1 < VMAX ? v[i + 1] : 0.0f;
+                const float2 a = make_float2(a0, a1);
+                const float2 b = make_float2(__shfl_down_sync(kFull, a0, 8), __shfl_down_sync(kFull, a1, 8));
+                const float2 c = make_float2(__shfl_down_sync(kFull, a0, 16), __shfl_down_sync(kFull, a1, 16));
+                const float2 d = make_float2(__shfl_down_sync(kFull, a0, 24), __shfl_down_sync(kFull, a1, 24));
+                const float2 s1 = __fadd2_rn(a, __fadd2_rn(__fadd2_rn(b, c), d));
+                if (lane < 8) {
+                    sm.part[i * 64 + 8 * warp + lane] = s1.x;
+                    if (i + 1 < n) sm.part[(i + 1) * 64 + 8 * warp + lane] = s1.y;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < VMAX; ++i) {
+            if (i < n) {
+                const float a = v[i];
+                const float b = __shfl_down_sync(kFull, a, 8);
+                const float c = __shfl_down_sync(kFull, a, 16);
+                const float d = __shfl_down_sync(kFull, a, 24);
+                const int op = i < split ? OP_A : OP_B;
+                float s1;
+                if (op == 0) s1 = a + ((b + c) + d);                               // bmfr.cl:33
+                else if (op == 1) s1 = fmin_cl(fmin_cl(fmin_cl(a, b), c), d);    // bmfr.cl:52-53
+                else s1 = fmax_cl(fmax_cl(fmax_cl(a, b), c), d);                 // bmfr.cl:74-75
+                if (lane < 8) sm.part[i * 64 + 8 * warp + lane] = s1;
+            }
         }
     }
     __syncthreads();
@@ -106,16 +125,18 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
             s2 = acc;
         }
     }
-    // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right.
+    // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right,
+    // by lane 0 of the group from shared memory.
     if (warp < n) {   // warp-uniform: warps without a value skip
-        const int base = lane & ~7;
-        float r = __shfl_sync(kFull, s2, base);
+        if (vi < n) sm.part2[vi * 8 + j] = s2;
+        __syncwarp();
+        if (vi < n && j == 0) {
+            const float* p = sm.part2 + vi * 8;
+            float r = p[0];
 #pragma unroll
-        for (int m = 1; m < 8; ++m) {
-            const float x = __shfl_sync(kFull, s2, base + m);
-            r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
+            for (int m = 1; m < 8; ++m) r = op == 0 ? r + p[m] : (op == 1 ? fmin_cl(r, p[m]) : fmax_cl(r, p[m]));
+            sm.out[vi] = r;
         }
-        if (vi < n && j == 0) sm.out[vi] = r;
     }
     __syncthreads();
 }
@@ -205,6 +226,40 @@ __device__ __forceinline__ void fill_noise_table(float* table, int frame) {
     for (int e = threadIdx.x; e < kNoiseTableFloats; e += kLocal) table[e] = noise_table_value(e, frame);
 }
 
+// Packed FP32 (sm_100 FADD2/FMUL2/FFMA2): two independent IEEE operations,
+// each rounded exactly as the scalar form, in one instruction.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// add_noise_r on two values at once.
+__device__ __forceinline__ float2 add_noise_r2(float2 v, float2 r, NoiseConst c) {
+    const float2 hi = dup2(c.hi), lo = dup2(c.lo);
+    const float2 p = mul2(hi, r);
+    const float2 pe = fma2(hi, r, neg2(p));
+    const float2 pl = fma2(lo, r, pe);
+    const float2 sm = add2(v, p);
+    const float2 bv = add2(sm, neg2(v));
+    const float2 se = add2(add2(v, neg2(add2(sm, neg2(bv)))), add2(p, neg2(bv)));
+    return add2(sm, add2(se, pl));
+}
+
+// Column k of the tile as two float pairs (rows q0,q1 and q2,q3), with the
+// first column's noise added to features 1..9 (bmfr.cl:625-627).
+template <bool HALF, bool NOISE>
+__device__ __forceinline__ void load_column(const Tile<HALF>& t, int k, int fb, const float* __restrict__ noise,
+                                            NoiseConst nc, float2& a01, float2& a23) {
+    a01 = t.get2(k, 0);
+    a23 = t.get2(k, 1);
+    if (NOISE && fb < kFeatures) {
+        const float* r = noise + (fb - 1) * 4 * kLocal + threadIdx.x;
+        a01 = add_noise_r2(a01, make_float2(r[0], r[kLocal]), nc);
+        a23 = add_noise_r2(a23, make_float2(r[2 * kLocal], r[3 * kLocal]), nc);
+    }
+}
+
 // One Householder column (bmfr.cl:549-655) on tile column 0; later columns
 // are tile columns 1..V.  NOISE: the first column, whose dot products read
 // features 1..9 with noise added (bmfr.cl:625-627).
@@ -213,18 +268,17 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
                                           NoiseConst nc, FitterSmem& sm) {
     const int V = kBuffers - 1 - col;
     const float2 c01 = t.get2(0, 0), c23 = t.get2(0, 1);
-    const float c[4] = {c01.x, c01.y, c23.x, c23.y};
     // Norm of rows >= col+1 (bmfr.cl:553-569); only row id (q = 0) can be above.
     float nv[1];
     {
         float s = 0.0f;
-        if (id >= col + 1) s = s + c[0] * c[0];
-        s = s + c[1] * c[1];
-        s = s + c[2] * c[2];
-        s = s + c[3] * c[3];
+        if (id >= col + 1) s = s + c01.x * c01.x;
+        s = s + c01.y * c01.y;
+        s = s + c23.x * c23.x;
+        s = s + c23.y * c23.y;
         nv[0] = s;
     }
-    if (id == col) sm.ucl = c[0];
+    if (id == col) sm.ucl = c01.x;
     block_reduce<1, 0, 0>(nv, 1, 1, sm);
     const float norm2 = sm.out[0];
     const float ucl = sm.ucl;
@@ -232,30 +286,30 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     const float vl = sqrtf(norm2 + ucl * ucl);
     const float ucl_new = ucl - vl;
     const float uls = norm2 + ucl_new * ucl_new;
-    if (id < col) sm.Rm[col][id] = c[0];
+    if (id < col) sm.Rm[col][id] = c01.x;
     if (id == col) sm.Rm[col][col] = vl;
-    float u[4] = {c[0], c[1], c[2], c[3]};
-    if (id == col) u[0] = ucl_new;
+    const float u0 = id == col ? ucl_new : c01.x;
     const bool row0 = id >= col;
+    // Rows below the column (only row id can be) take no part in the dot:
+    // 0 + a*0 leaves the reference's partial sum 0 unchanged.
+    const float2 uq0 = dup2(row0 ? u0 : 0.0f), uq1 = dup2(c01.y), uq2 = dup2(c23.x), uq3 = dup2(c23.y);
 
-    // Dot products with the later columns (bmfr.cl:606-638).
+    // Dot products with the later columns (bmfr.cl:606-638), two columns at
+    // a time in packed lanes; each lane keeps the reference's order.
     float d[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) {
-        d[i] = 0.0f;
+    for (int i = 0; i < 12; i += 2) {
+        d[i] = d[i + 1] = 0.0f;
         if (i < V) {
-            const float2 a01 = t.get2(i + 1, 0), a23 = t.get2(i + 1, 1);
-            float a[4] = {a01.x, a01.y, a23.x, a23.y};
-            if (NOISE && i + 1 < kFeatures) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], noise[(i * 4 + q) * kLocal + threadIdx.x], nc);
-            }
-            float s = 0.0f;
-            if (row0) s = s + a[0] * u[0];
-            s = s + a[1] * u[1];
-            s = s + a[2] * u[2];
-            s = s + a[3] * u[3];
-            d[i] = s;
+            float2 a01, a23, b01, b23;
+            load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
+            load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
+            float2 s = add2(dup2(0.0f), mul2(make_float2(a01.x, b01.x), uq0));
+            s = add2(s, mul2(make_float2(a01.y, b01.y), uq1));
+            s = add2(s, mul2(make_float2(a23.x, b23.x), uq2));
+            s = add2(s, mul2(make_float2(a23.y, b23.y), uq3));
+            d[i] = s.x;
+            d[i + 1] = s.y;
         }
     }
     block_reduce<12, 0, 0>(d, V, V, sm);
@@ -263,46 +317,41 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
     // Quotients take Markstein's correction when every operand is in range:
     // |u| and |dot| within [2^-32, 2^30] (or zero) and |u|^2 within 2^+-60
-    // keep numerator and quotient normal.
+    // keep numerator and quotient normal.  a - RN(num/uls) is formed as
+    // a + fma(-r, y, -q0), which keeps the sign of zero quotients exact.
     const float y = __frcp_rn(uls);
     const bool fast_b = uls >= 0x1p-60f && uls <= 0x1p60f;
-    const float u2[4] = {2.0f * u[0], 2.0f * u[1], 2.0f * u[2], 2.0f * u[3]};
+    const float2 u2_01 = make_float2(2.0f * u0, 2.0f * c01.y), u2_23 = make_float2(2.0f * c23.x, 2.0f * c23.y);
     bool fast_u = fast_b;
+    {
+        const float m[4] = {fabsf(u2_01.x), fabsf(u2_01.y), fabsf(u2_23.x), fabsf(u2_23.y)};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const float a = fabsf(u2[q]);
-        fast_u = fast_u && (a == 0.0f || (a >= 0x1p-32f && a <= 0x1p30f));
+        for (int q = 0; q < 4; ++q) fast_u = fast_u && (m[q] == 0.0f || (m[q] >= 0x1p-32f && m[q] <= 0x1p30f));
     }
+    const float2 ny = dup2(-y), b2 = dup2(uls);
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
         if (i < V) {
             const float dot = sm.out[i];
             const float ad = fabsf(dot);
             const bool fast = fast_u && (ad == 0.0f || (ad >= 0x1p-32f && ad <= 0x1p30f));
-            const float2 a01 = t.get2(i + 1, 0), a23 = t.get2(i + 1, 1);
-            float a[4] = {a01.x, a01.y, a23.x, a23.y};
-            if (NOISE && i + 1 < kFeatures) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = add_noise_r(a[q], noise[(i * 4 + q) * kLocal + threadIdx.x], nc);
-            }
-            float n[4];
+            float2 a01, a23;
+            load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
+            float2 n01, n23;
             if (fast) {
-                // a - RN(num / uls) as a + (-q1): the negated form keeps the
-                // sign of zero quotients exact without a select.
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float num = u2[q] * dot;
-                    const float q0 = num * y;
-                    const float r = __fmaf_rn(-q0, uls, num);
-                    n[q] = a[q] + __fmaf_rn(-r, y, -q0);
-                }
+                const float2 d2 = dup2(dot);
+                const float2 num01 = mul2(u2_01, d2), num23 = mul2(u2_23, d2);
+                const float2 nq01 = mul2(num01, ny), nq23 = mul2(num23, ny);
+                const float2 r01 = fma2(nq01, b2, num01), r23 = fma2(nq23, b2, num23);
+                n01 = add2(a01, fma2(r01, ny, nq01));
+                n23 = add2(a23, fma2(r23, ny, nq23));
             } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) n[q] = a[q] - div_slow(u2[q] * dot, uls);
+                n01 = make_float2(a01.x - div_slow(u2_01.x * dot, uls), a01.y - div_slow(u2_01.y * dot, uls));
+                n23 = make_float2(a23.x - div_slow(u2_23.x * dot, uls), a23.y - div_slow(u2_23.y * dot, uls));
             }
-            if (!row0) n[0] = a[0];
-            t.set2(i + 1, 0, n[0], n[1]);
-            t.set2(i + 1, 1, n[2], n[3]);
+            if (!row0) n01.x = a01.x;
+            t.set2(i + 1, 0, n01.x, n01.y);
+            t.set2(i + 1, 1, n23.x, n23.y);
         }
     }
     t.shift();
@@ -355,32 +404,44 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
         sm.rhs[id][2] = t.get2(2, 0).x;
     }
     __syncthreads();
-    // Back substitution (bmfr.cl:659-699): warp c solves colour channel c,
-    // lane x owning column x of R.
+    // Back substitution (bmfr.cl:659-699): warp c solves colour channel c.
+    // Lane x holds column x of R in registers, col[y] = R(x, y) for y <= x;
+    // lane 10 holds the right-hand side; the other lanes hold zeros.  Each
+    // step of the reference's work-group loop becomes shuffles within the warp.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp < 3) {
         const int c = warp;
-        float(*R)[12] = sm.Rb[c];
-        if (lane < kFeatures)
-            for (int y = 0; y <= lane; ++y) R[lane][y] = sm.Rm[lane][y];
-        if (lane == kFeatures)
-            for (int y = 0; y < kFeatures; ++y) R[kFeatures][y] = sm.rhs[y][c];
-        __syncwarp();
-        for (int i = kREdge - 2; i >= 0; --i) {
-            const float dv = R[i][i];
-            __syncwarp();
-            if (lane >= i && lane < kREdge) R[lane][i] = R[lane][i] / dv;
-            __syncwarp();
-            if (lane == kREdge - 1) {
-                float v = R[kREdge - 1][i];
-                for (int jj = i + 1; jj < kREdge - 1; ++jj) v = v - R[jj][i];
-                R[kREdge - 1][i] = v;
-            }
-            __syncwarp();
-            if (lane <= i) R[i][lane] = R[i][lane] * R[kREdge - 1][i];
-            __syncwarp();
+        float col[kFeatures];
+#pragma unroll
+        for (int y = 0; y < kFeatures; ++y) {
+            float v = 0.0f;
+            if (lane < kFeatures && y <= lane) v = sm.Rm[lane][y];
+            if (lane == kFeatures) v = sm.rhs[y][c];
+            col[y] = v;
         }
-        if (lane < kFeatures) weights_out[3 * lane + c] = R[kREdge - 1][lane];
+#pragma unroll
+        for (int i = kREdge - 2; i >= 0; --i) {
+            const float dv = __shfl_sync(kFull, col[i], i);               // R(i, i)
+            if (lane >= i && lane < kREdge) col[i] = col[i] / dv;        // R(x, i) /= R(i, i), x = i..10
+            float sub[kFeatures];
+#pragma unroll
+            for (int j = i + 1; j < kREdge - 1; ++j) sub[j] = __shfl_sync(kFull, col[i], j);
+            if (lane == kREdge - 1) {                                    // R(10, i) -= R(j, i), j = i+1..9
+                float v = col[i];
+#pragma unroll
+                for (int j = i + 1; j < kREdge - 1; ++j) v = v - sub[j];
+                col[i] = v;
+            }
+            const float xi = __shfl_sync(kFull, col[i], kREdge - 1);      // R(10, i), solved
+            if (lane == i) {                                             // R(i, y) *= R(10, i), y <= i
+#pragma unroll
+                for (int y = 0; y <= i; ++y) col[y] = col[y] * xi;
+            }
+        }
+        if (lane == kREdge - 1) {
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k) weights_out[3 * k + c] = col[k];
+        }
     }
     __syncthreads();
 }

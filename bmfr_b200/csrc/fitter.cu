@@ -30,7 +30,7 @@ struct FitterShared {
 };
 
 template <bool HALF_TMP, bool ROUND, bool NOISE_GLOBAL>
-__global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? (NOISE_GLOBAL ? 4 : 3) : 2)
+__global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
     k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, float* __restrict__ weights,
              float* __restrict__ mins_maxs, const float* __restrict__ noise_g, int* __restrict__ status) {
     using Shared = FitterShared<HALF_TMP, NOISE_GLOBAL>;
