@@ -20,7 +20,7 @@ from ._native import (BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, Scen
 
 __all__ = [
     "Plan", "Scene", "BmfrError", "default_params", "block_offsets",
-    "accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa",
+    "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
     "PIPELINE_FUSED", "PIPELINE_STAGED", "library_path",
 ]
 
@@ -237,6 +237,14 @@ def fitter(plan: Plan, weights, mins_maxs, tmp_data, frame_number: int, stream=N
                           _ptr(mins_maxs, "mins_maxs", plan.sizes.mins_maxs_bytes),
                           _ptr(tmp_data, "tmp_data", plan.sizes.tmp_data_bytes), int(frame_number),
                           _stream_ptr(stream)), "fitter")
+
+
+def fitter_fp64(plan: Plan, weights64, mins_maxs, tmp_data, frame_number: int, stream=None) -> None:
+    """The fitter in double precision (weights64: float64, blocks*10*3)."""
+    check(lib.bmfr_fitter_fp64(plan.handle, _ptr(weights64, "weights64", plan.sizes.weights_bytes * 2),
+                               _ptr(mins_maxs, "mins_maxs", plan.sizes.mins_maxs_bytes),
+                               _ptr(tmp_data, "tmp_data", plan.sizes.tmp_data_bytes), int(frame_number),
+                               _stream_ptr(stream)), "fitter_fp64")
 
 
 def weighted_sum(plan: Plan, weights, mins_maxs, output, current_normals, current_positions, current_noisy,

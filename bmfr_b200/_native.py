@@ -103,6 +103,7 @@ def _load() -> C.CDLL:
         "bmfr_block_offsets": (i, [C.POINTER(C.c_int)]),
         "bmfr_accumulate_noisy_data": (i, [vp, vp, u8p, vp, vp, vp, vp, vp, vp, u8p, u8p, vp, fp, fp, i, vp]),
         "bmfr_fitter": (i, [vp, vp, vp, vp, i, vp]),
+        "bmfr_fitter_fp64": (i, [vp, vp, vp, vp, i, vp]),
         "bmfr_fitter_noalloc": (i, [C.POINTER(Params), i, i, vp, vp, vp, i, vp]),
         "bmfr_weighted_sum": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp]),
         "bmfr_accumulate_filtered_data": (i, [vp, vp, vp, u8p, vp, vp, u8p, vp, vp, i, vp]),

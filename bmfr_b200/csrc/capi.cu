@@ -177,8 +177,6 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
     if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
         return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
-    if (params->half_history && params->pipeline != BMFR_PIPELINE_FUSED)
-        return fail(BMFR_E_UNSUPPORTED, "binary16 histories need the fused pipeline");
     if (params->pipeline != BMFR_PIPELINE_STAGED && params->pipeline != BMFR_PIPELINE_FUSED)
         return fail(BMFR_E_INVALID, "unknown pipeline");
     if (!(params->blend_alpha > 0.f) || !(params->second_blend_alpha > 0.f))
@@ -282,7 +280,7 @@ int bmfr_accumulate_noisy_data(const bmfr_plan* plan, float* out_prev_frame_pixe
     cudaError_t e = bmfr::launch_accumulate_noisy(
         plan->g, a, reinterpret_cast<float2*>(out_prev_frame_pixel), accept_bools, current_normals,
         previous_normals, current_positions, previous_positions, current_noisy, current_noisy, previous_noisy,
-        previous_spp, current_spp, tmp_data, (cudaStream_t)stream);
+        false, previous_spp, current_spp, tmp_data, (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "accumulate_noisy_data launch");
 }
 
@@ -298,6 +296,17 @@ int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const v
                                         plan->p.fp32_qr != 0, weights, mins_maxs, nullptr, plan->dev_status,
                                         (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
+}
+
+int bmfr_fitter_fp64(const bmfr_plan* plan, double* weights, float* mins_maxs, const void* tmp_data,
+                     int frame_number, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (!weights || !mins_maxs || !tmp_data) return fail(BMFR_E_INVALID, "fitter_fp64: NULL buffer");
+    if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter_fp64: negative frame number");
+    cudaError_t e = bmfr::launch_fitter_fp64(plan->g, frame_number, plan->p.noise_amount, tmp_data,
+                                             plan->p.use_half_precision_in_tmp_data != 0, weights, mins_maxs,
+                                             (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter_fp64 launch");
 }
 
 int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height, float* weights, float* mins_maxs,
@@ -434,7 +443,7 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     } else {
         if (e == cudaSuccess)
             e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
-                                              noisy, (float*)plan->noisy_acc[cur], (const float*)plan->noisy_acc[prv],
+                                              noisy, plan->noisy_acc[cur], plan->noisy_acc[prv], half_hist,
                                               plan->spp[prv], plan->spp[cur], plan->tmp, s);
         mark(1);
         if (e == cudaSuccess)
@@ -442,14 +451,22 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
                                     plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->noise_table,
                                     plan->dev_status, s);
         mark(2);
-        split = true;
-        if (e == cudaSuccess)
-            e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
-        mark(3);
-        if (e == cudaSuccess)
-            e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered, plan->prev_pix,
-                                                 plan->accept, albedo, plan->tone_mapped, plan->spp[cur],
-                                                 (const float*)plan->acc_filt[prv], (float*)plan->acc_filt[cur], s);
+        if (!half_hist) {
+            split = true;
+            if (e == cudaSuccess)
+                e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
+            mark(3);
+            if (e == cudaSuccess)
+                e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered,
+                                                     plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
+                                                     plan->spp[cur], (const float*)plan->acc_filt[prv],
+                                                     (float*)plan->acc_filt[cur], s);
+        } else if (e == cudaSuccess) {
+            e = bmfr::launch_weighted_sum_accumulate(g, f, plan->p.second_blend_alpha, plan->weights,
+                                                     plan->mins_maxs, cur_n, cur_p, plan->filtered, plan->prev_pix,
+                                                     plan->accept, albedo, plan->tone_mapped, plan->spp[cur],
+                                                     plan->acc_filt[prv], plan->acc_filt[cur], true, s);
+        }
     }
     if (!split) mark(3);
     mark(4);

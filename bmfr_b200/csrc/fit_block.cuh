@@ -357,9 +357,86 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     t.shift();
 }
 
+// The precision form's column (FP32 QR): the same reflections and reduction
+// trees with the block kept in float, fused multiply-adds in the dot
+// products and updates, and the update written as a - u * (2 dot / |u|^2).
+// It no longer rounds like the reference; it is checked against the fp64
+// fitter instead.
+template <bool NOISE>
+__device__ __forceinline__ void qr_column_fast(Tile<false>& t, int col, int id, const float* __restrict__ noise,
+                                               NoiseConst nc, FitterSmem& sm) {
+    const int V = kBuffers - 1 - col;
+    const float c0 = t.f[0][0], c1 = t.f[0][1], c2 = t.f[0][2], c3 = t.f[0][3];
+    float nv[1];
+    {
+        float s = (id >= col + 1) ? c0 * c0 : 0.0f;
+        s = __fmaf_rn(c1, c1, s);
+        s = __fmaf_rn(c2, c2, s);
+        s = __fmaf_rn(c3, c3, s);
+        nv[0] = s;
+    }
+    if (id == col) sm.ucl = c0;
+    block_reduce<1, 0, 0>(nv, 1, 1, sm);
+    const float norm2 = sm.out[0];
+    const float ucl = sm.ucl;
+    const float vl = sqrtf(__fmaf_rn(ucl, ucl, norm2));
+    const float ucl_new = ucl - vl;
+    const float uls = __fmaf_rn(ucl_new, ucl_new, norm2);
+    if (id < col) sm.Rm[col][id] = c0;
+    if (id == col) sm.Rm[col][col] = vl;
+    const bool row0 = id >= col;
+    const float u0 = id == col ? ucl_new : c0;
+    const float2 uq0 = dup2(row0 ? u0 : 0.0f), uq1 = dup2(c1), uq2 = dup2(c2), uq3 = dup2(c3);
+    const float2 hi = dup2(nc.hi);
+    auto column = [&](int k, float2& a01, float2& a23) {
+        a01 = make_float2(t.f[k][0], t.f[k][1]);
+        a23 = make_float2(t.f[k][2], t.f[k][3]);
+        if (NOISE && k < kFeatures) {
+            const float* r = noise + (k - 1) * 4 * kLocal + threadIdx.x;
+            a01 = fma2(hi, make_float2(r[0], r[kLocal]), a01);
+            a23 = fma2(hi, make_float2(r[2 * kLocal], r[3 * kLocal]), a23);
+        }
+    };
+    float d[12];
+#pragma unroll
+    for (int i = 0; i < 12; i += 2) {
+        d[i] = d[i + 1] = 0.0f;
+        if (i < V) {
+            float2 a01, a23, b01, b23;
+            column(i + 1, a01, a23);
+            column(i + 2, b01, b23);
+            float2 sacc = mul2(make_float2(a01.x, b01.x), uq0);
+            sacc = fma2(make_float2(a01.y, b01.y), uq1, sacc);
+            sacc = fma2(make_float2(a23.x, b23.x), uq2, sacc);
+            sacc = fma2(make_float2(a23.y, b23.y), uq3, sacc);
+            d[i] = sacc.x;
+            d[i + 1] = sacc.y;
+        }
+    }
+    block_reduce<12, 0, 0>(d, V, V, sm);
+    const float y2 = 2.0f * __frcp_rn(uls);
+    const float2 nu01 = make_float2(row0 ? -u0 : 0.0f, -c1), nu23 = make_float2(-c2, -c3);
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        if (i < V) {
+            const float2 w = dup2(sm.out[i] * y2);
+            float2 a01, a23;
+            column(i + 1, a01, a23);
+            a01 = fma2(nu01, w, a01);
+            a23 = fma2(nu23, w, a23);
+            t.f[i + 1][0] = a01.x;
+            t.f[i + 1][1] = a01.y;
+            t.f[i + 1][2] = a23.x;
+            t.f[i + 1][3] = a23.y;
+        }
+    }
+    t.shift();
+}
+
 // Fits one block held in t (the values as loaded from tmp_data) and writes
 // its 30 weights and 12 min/max values.  Ends with a barrier.
-template <bool HALF>
+// FAST (float tile only): the precision form's FP32 QR (qr_column_fast).
+template <bool HALF, bool FAST = false>
 __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict__ noise, NoiseConst nc,
                                           FitterSmem& sm, float* __restrict__ weights_out,
                                           float* __restrict__ mm_out) {
@@ -392,9 +469,15 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
         t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
     }
 
-    qr_column<HALF, true>(t, 0, id, noise, nc, sm);
+    if constexpr (FAST && !HALF) {
+        qr_column_fast<true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1
-    for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);
+        for (int col = 1; col < kFeatures; ++col) qr_column_fast<false>(t, col, id, noise, nc, sm);
+    } else {
+        qr_column<HALF, true>(t, 0, id, noise, nc, sm);
+#pragma unroll 1
+        for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);
+    }
 
     // After ten shifts the colour columns are tile columns 0..2: rows 0..9
     // form R's right-hand side (bmfr.cl:596-600 for col >= 10).

@@ -87,7 +87,9 @@ __global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
             mbar_arrive_expect_tx(&S.bar, kTileBytes);
             bulk_copy_g2s(S.tile, src + (size_t)next * kTileBytes, kTileBytes, &S.bar);
         }
-        fit_block<ROUND>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3, mins_maxs + (size_t)b * kScaled * 2);
+        // HALF_TMP without ROUND is the precision form (fp32_qr): FP32 QR.
+        fit_block<ROUND, HALF_TMP && !ROUND>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3,
+                                             mins_maxs + (size_t)b * kScaled * 2);
     }
 }
 

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256, 3) k_fused_block(
     }
 
     // Phase 2: the fit; weights and min/max stay in shared memory.
-    fit_block<ROUND>(t, noise, nc, sm, w_s, mm_s);
+    fit_block<ROUND, HALF_TMP && !ROUND>(t, noise, nc, sm, w_s, mm_s);
     if (threadIdx.x < kFeatures * 3) weights[(size_t)b * kFeatures * 3 + threadIdx.x] = w_s[threadIdx.x];
     if (threadIdx.x < kScaled * 2) mins_maxs[(size_t)b * kScaled * 2 + threadIdx.x] = mm_s[threadIdx.x];
 

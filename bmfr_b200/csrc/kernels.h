@@ -8,11 +8,16 @@
 
 namespace bmfr {
 
+// noisy_out/prev_noisy: the accumulated-colour history, float or (with
+// half_history) binary16; noisy_in == noisy_out runs the in-place form.
 cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float2* prev_pix, uint8_t* accept,
                                     const float* cur_n, const float* prev_n, const float* cur_p,
-                                    const float* prev_p, const float* noisy_in, float* noisy_out,
-                                    const float* prev_noisy, const uint8_t* prev_spp, uint8_t* cur_spp,
-                                    void* tmp, cudaStream_t s);
+                                    const float* prev_p, const float* noisy_in, void* noisy_out,
+                                    const void* prev_noisy, bool half_history, const uint8_t* prev_spp,
+                                    uint8_t* cur_spp, void* tmp, cudaStream_t s);
+// The fitter in double precision (precision form's reference).
+cudaError_t launch_fitter_fp64(const Geometry& g, int frame, double noise_amount, const void* tmp, bool half_tmp,
+                               double* weights, float* mins_maxs, cudaStream_t s);
 
 // status: device word that receives a nonzero code if a bounded wait ran out.
 // noise_table: the frame's table from launch_noise_table, or null to have

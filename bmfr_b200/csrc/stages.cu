@@ -20,12 +20,14 @@ namespace bmfr {
 // MODE 1: only in-image pixels, noisy_in == noisy_out (in-place, first pass);
 // MODE 2: only mirrored margin pixels, taking the colour their in-image pixel
 //         wrote in pass 1 (in-place, second pass).
-template <int MODE>
+// HistT: element type of the accumulated-colour history (noisy_out and
+// prev_noisy); in-place modes use float.
+template <int MODE, typename HistT>
 __global__ void __launch_bounds__(256) k_accumulate_noisy(
     Geometry g, AccumArgs a, float2* __restrict__ prev_pix, uint8_t* __restrict__ accept,
     const float* __restrict__ cur_n, const float* __restrict__ prev_n,
     const float* __restrict__ cur_p, const float* __restrict__ prev_p,
-    const float* noisy_in, float* noisy_out, const float* __restrict__ prev_noisy,
+    const float* noisy_in, HistT* noisy_out, const HistT* __restrict__ prev_noisy,
     const uint8_t* __restrict__ prev_spp, uint8_t* __restrict__ cur_spp, void* __restrict__ tmp) {
     const int gx = blockIdx.x * 32 + threadIdx.x;
     const int gy = blockIdx.y * 8 + threadIdx.y;
@@ -40,15 +42,15 @@ __global__ void __launch_bounds__(256) k_accumulate_noisy(
     const float3 wp = load3(cur_p, lp);
     const float3 nrm = load3(cur_n, lp);
     if (MODE == 2) {
-        store_tmp_row(g, tmp, a.use_half, gx, gy, wp, nrm, load3(noisy_out, lp));
+        store_tmp_row(g, tmp, a.use_half, gx, gy, wp, nrm, hist_load(noisy_out, lp));
         return;
     }
     const float3 cur = load3(noisy_in, lp);
-    const AccumResult r = accumulate_core<float>(g, a, px, py, wp, nrm, cur, prev_n, prev_p, prev_noisy, prev_spp);
+    const AccumResult r = accumulate_core<HistT>(g, a, px, py, wp, nrm, cur, prev_n, prev_p, prev_noisy, prev_spp);
     store_tmp_row(g, tmp, a.use_half, gx, gy, wp, nrm, r.color);
     if (in_image) {   // bmfr.cl:442, 478-484
         cur_spp[lp] = r.spp;
-        store3(noisy_out, lp, r.color);
+        hist_store(noisy_out, lp, r.color);
         prev_pix[lp] = make_float2(r.ppx, r.ppy);
         accept[lp] = r.accept;
     }
@@ -141,23 +143,28 @@ __global__ void __launch_bounds__(256) k_taa(Geometry g, int frame, float taa_al
 static dim3 margin_grid(const Geometry& g) { return dim3(g.MW / 32, g.MH / 8); }
 static dim3 image_grid(const Geometry& g) { return dim3((g.W + 31) / 32, (g.H + 7) / 8); }
 
-cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float2* prev_pix,
-                                    uint8_t* accept, const float* cur_n, const float* prev_n,
-                                    const float* cur_p, const float* prev_p, const float* noisy_in,
-                                    float* noisy_out, const float* prev_noisy, const uint8_t* prev_spp,
+cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float2* prev_pix, uint8_t* accept,
+                                    const float* cur_n, const float* prev_n, const float* cur_p,
+                                    const float* prev_p, const float* noisy_in, void* noisy_out,
+                                    const void* prev_noisy, bool half_history, const uint8_t* prev_spp,
                                     uint8_t* cur_spp, void* tmp, cudaStream_t s) {
     const dim3 block(32, 8);
-    if (noisy_in == noisy_out) {
-        k_accumulate_noisy<1><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
-                                                               prev_p, noisy_in, noisy_out, prev_noisy,
-                                                               prev_spp, cur_spp, tmp);
-        k_accumulate_noisy<2><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
-                                                               prev_p, noisy_in, noisy_out, prev_noisy,
-                                                               prev_spp, cur_spp, tmp);
+    if (half_history) {
+        k_accumulate_noisy<0, __half><<<margin_grid(g), block, 0, s>>>(
+            g, a, prev_pix, accept, cur_n, prev_n, cur_p, prev_p, noisy_in, (__half*)noisy_out,
+            (const __half*)prev_noisy, prev_spp, cur_spp, tmp);
+    } else if (noisy_in == noisy_out) {
+        float* io = (float*)noisy_out;
+        k_accumulate_noisy<1, float><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
+                                                                      prev_p, noisy_in, io, (const float*)prev_noisy,
+                                                                      prev_spp, cur_spp, tmp);
+        k_accumulate_noisy<2, float><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
+                                                                      prev_p, noisy_in, io, (const float*)prev_noisy,
+                                                                      prev_spp, cur_spp, tmp);
     } else {
-        k_accumulate_noisy<0><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
-                                                               prev_p, noisy_in, noisy_out, prev_noisy,
-                                                               prev_spp, cur_spp, tmp);
+        k_accumulate_noisy<0, float><<<margin_grid(g), block, 0, s>>>(
+            g, a, prev_pix, accept, cur_n, prev_n, cur_p, prev_p, noisy_in, (float*)noisy_out,
+            (const float*)prev_noisy, prev_spp, cur_spp, tmp);
     }
     return cudaGetLastError();
 }

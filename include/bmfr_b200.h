@@ -150,6 +150,13 @@ int bmfr_accumulate_noisy_data(const bmfr_plan* plan,
 int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs,
                 const void* tmp_data, int frame_number, void* stream);
 
+/* The fitter in double precision, the reference arithmetic of the
+ * precision form (params.fp32_qr): same steps, reduction trees and noise as
+ * bmfr_fitter, every value in double and no intermediate rounding.  weights:
+ * blocks * 10 * 3 doubles.  The only FP64 code on the device. */
+int bmfr_fitter_fp64(const bmfr_plan* plan, double* weights, float* mins_maxs,
+                     const void* tmp_data, int frame_number, void* stream);
+
 /* bmfr_fitter without any device allocation; no counterpart in the
  * reference.  For callers that cannot call cudaMalloc: renderers whose engine
  * owns all device memory under a fixed budget, and per-frame code that cannot
