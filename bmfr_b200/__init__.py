@@ -15,11 +15,11 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import (BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check, lib,
-                      PIPELINE_FUSED, PIPELINE_STAGED)
+from ._native import (BatchTuning, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check,
+                      lib, PIPELINE_FUSED, PIPELINE_STAGED)
 
 __all__ = [
-    "Plan", "Scene", "BmfrError", "default_params", "block_offsets",
+    "Plan", "Batch", "Scene", "BmfrError", "default_params", "block_offsets",
     "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
     "PIPELINE_FUSED", "PIPELINE_STAGED", "library_path",
 ]
@@ -286,6 +286,128 @@ def taa(plan: Plan, in_prev_frame_pixel, new_frame, result_frame, prev_frame, fr
                        _stream_ptr(stream)), "taa")
 
 
+# -- many streams (include/bmfr_batch.h) -------------------------------------
+
+class Batch:
+    """Many streams of uneven size denoised together, one CUDA graph per step."""
+
+    def __init__(self, params: Params | None = None, memory_budget_bytes: int = 0, **overrides):
+        self.params = params if params is not None else default_params(**overrides)
+        h = C.c_void_p()
+        check(lib.bmfr_batch_create(C.byref(self.params), int(memory_budget_bytes), C.byref(h)), "bmfr_batch_create")
+        self._h = h
+        self.sizes = {}
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise BmfrError(_native.BMFR_E_STATE, "batch destroyed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib.bmfr_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def stream_bytes(params: Params, width: int, height: int, own_inputs: bool = False) -> int:
+        n = C.c_size_t()
+        check(lib.bmfr_batch_stream_bytes(C.byref(params), width, height, int(own_inputs), C.byref(n)),
+              "bmfr_batch_stream_bytes")
+        return n.value
+
+    def add_stream(self, width: int, height: int, own_inputs: bool = False) -> int:
+        slot = C.c_int()
+        check(lib.bmfr_batch_add_stream(self.handle, int(width), int(height), int(own_inputs), C.byref(slot)),
+              "bmfr_batch_add_stream")
+        self.sizes[slot.value] = (int(width), int(height))
+        return slot.value
+
+    def remove_stream(self, slot: int) -> None:
+        check(lib.bmfr_batch_remove_stream(self.handle, int(slot)), "bmfr_batch_remove_stream")
+        self.sizes.pop(slot, None)
+
+    def reset_stream(self, slot: int) -> None:
+        check(lib.bmfr_batch_reset_stream(self.handle, int(slot)), "bmfr_batch_reset_stream")
+
+    def frame(self, slot: int) -> int:
+        v = lib.bmfr_batch_stream_frame(self.handle, int(slot))
+        if v < 0:
+            check(v, "bmfr_batch_stream_frame")
+        return v
+
+    @property
+    def bytes_in_use(self) -> int:
+        return lib.bmfr_batch_bytes_in_use(self.handle)
+
+    def stream_inputs(self, slot: int) -> FrameInputs:
+        fi = FrameInputs()
+        check(lib.bmfr_batch_stream_inputs(self.handle, int(slot), C.byref(fi)), "bmfr_batch_stream_inputs")
+        return fi
+
+    @staticmethod
+    def frame_io(albedo, normals, positions, noisy, previous_normals=None, previous_positions=None,
+                 result=None) -> FrameIO:
+        """A FrameIO of device tensors (or raw device addresses)."""
+        return FrameIO(_ptr(albedo, "albedo"), _ptr(normals, "normals"), _ptr(positions, "positions"),
+                       _ptr(noisy, "noisy"), _ptr(previous_normals, "previous_normals", optional=True),
+                       _ptr(previous_positions, "previous_positions", optional=True),
+                       _ptr(result, "result", optional=True))
+
+    def _args(self, slots, io, matrices, offsets):
+        n = len(slots)
+        sl = (C.c_int * n)(*slots)
+        iop = None
+        if io is not None:
+            arr = (FrameIO * n)()
+            for k, v in enumerate(io):
+                arr[k] = v if v is not None else FrameIO()
+            iop = arr
+        m, mp = _f32(matrices, 16 * n, "matrices")
+        o, op = _f32(offsets, 2 * n, "offsets")
+        return n, sl, iop, (m, o), mp, op
+
+    def step(self, slots, matrices, offsets, io=None, stream=None) -> None:
+        """Denoises the next frame of each stream in `slots` (one graph launch)."""
+        n, sl, iop, keep, mp, op = self._args(slots, io, matrices, offsets)
+        check(lib.bmfr_batch_step(self.handle, n, sl, iop, mp, op, _stream_ptr(stream)), "bmfr_batch_step")
+
+    def result_ptr(self, slot: int) -> int:
+        p = C.c_void_p()
+        check(lib.bmfr_batch_stream_result(self.handle, int(slot), C.byref(p)), "bmfr_batch_stream_result")
+        return p.value
+
+    @property
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        check(lib.bmfr_batch_get_tuning(self.handle, C.byref(t)), "bmfr_batch_get_tuning")
+        return t
+
+    def set_tuning(self, block_ctas_per_sm=0, taa_tile_w=32, taa_tile_h=8, staging_depth=0) -> None:
+        t = BatchTuning(block_ctas_per_sm, taa_tile_w, taa_tile_h, staging_depth)
+        check(lib.bmfr_batch_set_tuning(self.handle, C.byref(t)), "bmfr_batch_set_tuning")
+
+    def autotune(self, slots, matrices, offsets, io=None, steps=3, stream=None):
+        n, sl, iop, keep, mp, op = self._args(slots, io, matrices, offsets)
+        t = BatchTuning()
+        ms = C.c_float()
+        check(lib.bmfr_batch_autotune(self.handle, n, sl, iop, mp, op, int(steps), _stream_ptr(stream),
+                                      C.byref(t), C.byref(ms)), "bmfr_batch_autotune")
+        return t, ms.value
+
+
 # -- input source ------------------------------------------------------------
 
 class Scene:
@@ -341,3 +463,11 @@ class Scene:
         if cl is not None:
             out["clean"] = cl
         return out
+
+    def render_device(self, frame: int, albedo, normals, positions, noisy, clean=None, stream=None) -> None:
+        """Renders frame `frame` on the GPU into device tensors (H*W*3 float32)."""
+        n = self.width * self.height * 12
+        check(lib.bmfr_scene_render_device(C.byref(self.desc), int(frame), _ptr(albedo, "albedo", n),
+                                           _ptr(normals, "normals", n), _ptr(positions, "positions", n),
+                                           _ptr(noisy, "noisy", n), _ptr(clean, "clean", n, optional=True),
+                                           _stream_ptr(stream)), "bmfr_scene_render_device")

@@ -74,6 +74,11 @@ class FrameIO(C.Structure):
                 ("previous_positions", C.c_void_p), ("result", C.c_void_p)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("block_ctas_per_sm", C.c_int), ("taa_tile_w", C.c_int), ("taa_tile_h", C.c_int),
+                ("staging_depth", C.c_int)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("width", C.c_int), ("height", C.c_int),
@@ -120,12 +125,28 @@ def _load() -> C.CDLL:
         "bmfr_plan_enable_profiling": (i, [vp, i]),
         "bmfr_plan_check_device": (i, [vp, vp]),
         "bmfr_plan_stage_times": (i, [vp, fp]),
+        "bmfr_batch_create": (i, [C.POINTER(Params), C.c_size_t, C.POINTER(vp)]),
+        "bmfr_batch_destroy": (i, [vp]),
+        "bmfr_batch_stream_bytes": (i, [C.POINTER(Params), i, i, i, C.POINTER(C.c_size_t)]),
+        "bmfr_batch_add_stream": (i, [vp, i, i, i, C.POINTER(i)]),
+        "bmfr_batch_remove_stream": (i, [vp, i]),
+        "bmfr_batch_reset_stream": (i, [vp, i]),
+        "bmfr_batch_stream_frame": (i, [vp, i]),
+        "bmfr_batch_bytes_in_use": (C.c_size_t, [vp]),
+        "bmfr_batch_stream_inputs": (i, [vp, i, C.POINTER(FrameInputs)]),
+        "bmfr_batch_step": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, vp]),
+        "bmfr_batch_stream_result": (i, [vp, i, C.POINTER(vp)]),
+        "bmfr_batch_get_tuning": (i, [vp, C.POINTER(BatchTuning)]),
+        "bmfr_batch_set_tuning": (i, [vp, C.POINTER(BatchTuning)]),
+        "bmfr_batch_autotune": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, i, vp,
+                                    C.POINTER(BatchTuning), C.POINTER(C.c_float)]),
         "bmfr_last_error": (C.c_char_p, []),
         "bmfr_status_string": (C.c_char_p, [i]),
         "bmfr_scene_default": (i, [C.POINTER(SceneDesc), C.c_uint64, i, i, i]),
         "bmfr_scene_camera": (i, [C.POINTER(SceneDesc), i, fp]),
         "bmfr_scene_pixel_offset": (i, [C.POINTER(SceneDesc), i, fp]),
         "bmfr_scene_render": (i, [C.POINTER(SceneDesc), i, fp, fp, fp, fp, fp, i]),
+        "bmfr_scene_render_device": (i, [C.POINTER(SceneDesc), i, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

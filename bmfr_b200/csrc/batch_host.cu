@@ -1,0 +1,502 @@
+// batch_host.cu — the many-stream engine of include/bmfr_batch.h: stream
+// slots with their HBM histories, the per-step description, the CUDA graph
+// of a step, and the autotuner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "batch.cuh"
+#include "bmfr_batch.h"
+#include "status.h"
+
+using bmfr::cuda_fail;
+using bmfr::fail;
+
+namespace {
+
+struct StreamSlot {
+    bool used = false;
+    int width = 0, height = 0;
+    bmfr::Geometry g{};
+    int frame = 0;
+    bool own_inputs = false;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+    // histories (HistT per the batch's half_history) and per-frame buffers
+    void* noisy_acc[2] = {nullptr, nullptr};
+    void* acc_filt[2] = {nullptr, nullptr};
+    void* result[2] = {nullptr, nullptr};
+    uint8_t* spp[2] = {nullptr, nullptr};
+    float2* prev_pix = nullptr;
+    uint8_t* accept = nullptr;
+    float* tone_mapped = nullptr;
+    float* result_f32 = nullptr;
+    float* weights = nullptr;
+    float* mins_maxs = nullptr;
+    float* noise = nullptr;
+    // own input slots
+    float* normals[2] = {nullptr, nullptr};
+    float* positions[2] = {nullptr, nullptr};
+    float* albedo = nullptr;
+    float* noisy = nullptr;
+};
+
+size_t stream_bytes(const bmfr_params& p, int w, int h, bool own_inputs) {
+    const bmfr::Geometry g = bmfr::make_geometry(w, h);
+    const size_t px = (size_t)w * h;
+    const size_t hist = px * 3 * (p.half_history ? 2 : 4);
+    size_t b = 6 * hist + 2 * px + px * 8 + px + px * 12 + px * 12;
+    b += (size_t)g.blocks * (bmfr::kFeatures * 3 + bmfr::kScaled * 2) * 4 + bmfr::kNoiseTableBytes;
+    if (own_inputs) b += px * 12 * 6;
+    return b;
+}
+
+}  // namespace
+
+struct bmfr_batch {
+    bmfr_params p{};
+    int device = 0;
+    int sms = 0;
+    size_t budget = 0, used = 0;
+    std::vector<StreamSlot> slots = std::vector<StreamSlot>(BMFR_BATCH_MAX_STREAMS);
+    bmfr::BatchTuning tuning{0, 32, 8, 0};
+    int block_occupancy = 1;
+    bmfr::BatchStepDesc* d_desc = nullptr;
+    bmfr::BatchStepDesc* h_desc[2] = {nullptr, nullptr};
+    int* d_counters = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    bool graphs_valid = false;
+    int next = 0;
+    int last = -1;
+};
+
+namespace {
+
+int check_batch(const bmfr_batch* b) {
+    if (!b) return fail(BMFR_E_INVALID, "batch is NULL");
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != b->device)
+        return fail(BMFR_E_STATE, "the current CUDA device is not the batch's device");
+    return BMFR_OK;
+}
+
+int check_slot(const bmfr_batch* b, int slot) {
+    if (slot < 0 || slot >= BMFR_BATCH_MAX_STREAMS || !b->slots[slot].used)
+        return fail(BMFR_E_NOT_FOUND, "no stream in slot " + std::to_string(slot));
+    return BMFR_OK;
+}
+
+void free_slot(bmfr_batch* b, StreamSlot& s) {
+    for (void* p : s.allocs) cudaFree(p);
+    b->used -= s.bytes;
+    s = StreamSlot();
+}
+
+void destroy_graphs(bmfr_batch* b) {
+    for (int k = 0; k < 2; ++k) {
+        if (b->graph[k]) cudaGraphExecDestroy(b->graph[k]);
+        b->graph[k] = nullptr;
+    }
+    b->graphs_valid = false;
+}
+
+// Captures the step: description upload, queue reset, noise tables, the
+// block queue and the TAA tiles.  One graph per pinned description buffer.
+int build_graphs(bmfr_batch* b) {
+    for (cudaEvent_t e : b->done)
+        if (e) cudaEventSynchronize(e);
+    destroy_graphs(b);
+    cudaStream_t cs;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "batch capture stream");
+    const bool half_tmp = b->p.use_half_precision_in_tmp_data != 0;
+    int ctas = b->tuning.block_ctas_per_sm > 0 ? std::min(b->tuning.block_ctas_per_sm, b->block_occupancy)
+                                               : b->block_occupancy;
+    ctas = std::max(ctas, 1);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) break;
+        e = cudaMemcpyAsync(b->d_desc, b->h_desc[k], sizeof(bmfr::BatchStepDesc), cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(int), cs);
+        if (e == cudaSuccess) e = bmfr::launch_batch_noise(b->d_desc, BMFR_BATCH_MAX_STREAMS, cs);
+        if (e == cudaSuccess)
+            e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr != 0, half_tmp,
+                                          b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms, cs);
+        if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[k], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        destroy_graphs(b);
+        return cuda_fail(e, "batch graph capture");
+    }
+    b->graphs_valid = true;
+    return BMFR_OK;
+}
+
+bmfr::AccumArgs step_args(const bmfr_batch* b, const float* m, const float* off, int frame) {
+    bmfr::AccumArgs a;
+    std::memcpy(a.m, m, sizeof a.m);
+    a.off_x = off[0];
+    a.off_y = off[1];
+    a.pos_lim2 = b->p.position_limit_squared;
+    a.nrm_lim2 = b->p.normal_limit_squared;
+    a.blend_alpha = b->p.blend_alpha;
+    a.frame = frame;
+    a.use_half = b->p.use_half_precision_in_tmp_data ? 1 : 0;
+    return a;
+}
+
+// Fills description buffer k for the listed streams.
+int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, const bmfr_frame_io* io,
+              const float* matrices, const float* offsets) {
+    const int tw = b->tuning.tile_w, th = b->tuning.tile_h;
+    int blocks = 0, tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        StreamSlot& s = b->slots[slots[i]];
+        const int f = s.frame, cur = f & 1, prv = cur ^ 1;
+        const bmfr_frame_io* fi = io ? &io[i] : nullptr;
+        const bool own = !fi || !fi->albedo;
+        if (own && !s.own_inputs)
+            return fail(BMFR_E_INVALID, "stream " + std::to_string(slots[i]) + " has no input slots; pass io");
+        bmfr::BatchStreamJob& J = d->s[i];
+        J.job.g = s.g;
+        J.job.a = step_args(b, matrices + 16 * i, offsets + 2 * i, f);
+        J.job.nc = bmfr::make_noise_const(b->p.noise_amount);
+        J.job.second_alpha = b->p.second_blend_alpha;
+        bmfr::FusedBuffers& fb = J.job.fb;
+        fb.cur_n = own ? s.normals[cur] : fi->normals;
+        fb.prev_n = own ? s.normals[prv] : fi->previous_normals;
+        fb.cur_p = own ? s.positions[cur] : fi->positions;
+        fb.prev_p = own ? s.positions[prv] : fi->previous_positions;
+        fb.noisy_in = own ? s.noisy : fi->noisy;
+        fb.albedo = own ? s.albedo : fi->albedo;
+        if (!fb.cur_n || !fb.cur_p || !fb.noisy_in || !fb.albedo)
+            return fail(BMFR_E_INVALID, "step: NULL input buffer");
+        if (f > 0 && (!fb.prev_n || !fb.prev_p))
+            return fail(BMFR_E_INVALID, "step: previous G-buffer missing");
+        if (!fb.prev_n) fb.prev_n = fb.cur_n;   // frame 0 reads no history
+        if (!fb.prev_p) fb.prev_p = fb.cur_p;
+        fb.noisy_acc_cur = s.noisy_acc[cur];
+        fb.noisy_acc_prev = s.noisy_acc[prv];
+        fb.prev_spp = s.spp[prv];
+        fb.cur_spp = s.spp[cur];
+        fb.prev_pix = s.prev_pix;
+        fb.accept = s.accept;
+        fb.tone_mapped = s.tone_mapped;
+        fb.acc_prev = s.acc_filt[prv];
+        fb.acc_cur = s.acc_filt[cur];
+        fb.weights = s.weights;
+        fb.mins_maxs = s.mins_maxs;
+        fb.noise = s.noise;
+        J.block_start = blocks;
+        J.tile_start = tiles;
+        J.tiles_x = (s.width + tw - 1) / tw;
+        J.taa_alpha = b->p.taa_blend_alpha;
+        J.result_hist = s.result[cur];
+        J.result_prev = s.result[prv];
+        J.result_out = (fi && fi->result) ? fi->result : s.result_f32;
+        blocks += s.g.blocks;
+        tiles += J.tiles_x * ((s.height + th - 1) / th);
+    }
+    d->n_streams = n;
+    d->n_blocks = blocks;
+    d->n_tiles = tiles;
+    d->tile_w = tw;
+    return BMFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bmfr_batch_stream_bytes(const bmfr_params* params, int width, int height, int own_inputs, size_t* bytes) {
+    if (!params || !bytes) return fail(BMFR_E_INVALID, "NULL argument");
+    *bytes = stream_bytes(*params, width, height, own_inputs != 0);
+    return BMFR_OK;
+}
+
+int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmfr_batch** out) {
+    if (!params || !out) return fail(BMFR_E_INVALID, "NULL argument");
+    *out = nullptr;
+    if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    int dev = -1;
+    if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "no CUDA device");
+    }
+    bmfr_batch* b = new bmfr_batch;
+    b->p = *params;
+    b->p.pipeline = BMFR_PIPELINE_FUSED;
+    b->device = dev;
+    b->budget = memory_budget_bytes;
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    b->block_occupancy = std::max(1, bmfr::batch_block_occupancy(params->fp32_qr != 0,
+                                                                 params->use_half_precision_in_tmp_data != 0,
+                                                                 params->half_history != 0));
+    cudaError_t e = cudaMalloc(&b->d_desc, sizeof(bmfr::BatchStepDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * sizeof(int));
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaMallocHost(&b->h_desc[k], sizeof(bmfr::BatchStepDesc));
+        if (e == cudaSuccess) std::memset(b->h_desc[k], 0, sizeof(bmfr::BatchStepDesc));
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done[k], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        bmfr_batch_destroy(b);
+        return cuda_fail(e, "batch allocation");
+    }
+    *out = b;
+    return BMFR_OK;
+}
+
+int bmfr_batch_destroy(bmfr_batch* b) {
+    if (!b) return BMFR_OK;
+    for (cudaEvent_t e : b->done)
+        if (e) cudaEventSynchronize(e);
+    destroy_graphs(b);
+    for (StreamSlot& s : b->slots)
+        if (s.used) free_slot(b, s);
+    for (int k = 0; k < 2; ++k) {
+        if (b->h_desc[k]) cudaFreeHost(b->h_desc[k]);
+        if (b->done[k]) cudaEventDestroy(b->done[k]);
+    }
+    if (b->d_desc) cudaFree(b->d_desc);
+    if (b->d_counters) cudaFree(b->d_counters);
+    delete b;
+    return BMFR_OK;
+}
+
+int bmfr_batch_add_stream(bmfr_batch* b, int width, int height, int own_inputs, int* slot) {
+    if (int st = check_batch(b)) return st;
+    if (!slot) return fail(BMFR_E_INVALID, "slot is NULL");
+    if (width < 32 || height < 32 || width > 16384 || height > 16384)
+        return fail(BMFR_E_INVALID, "image size must be within [32, 16384]");
+    const bmfr::Geometry g = bmfr::make_geometry(width, height);
+    if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
+        return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
+    int k = 0;
+    while (k < BMFR_BATCH_MAX_STREAMS && b->slots[k].used) ++k;
+    if (k == BMFR_BATCH_MAX_STREAMS) return fail(BMFR_E_TOO_LARGE, "all stream slots are in use");
+    const size_t bytes = stream_bytes(b->p, width, height, own_inputs != 0);
+    if (b->budget && b->used + bytes > b->budget)
+        return fail(BMFR_E_BUDGET, "stream needs " + std::to_string(bytes) + " bytes, " +
+                                       std::to_string(b->budget - b->used) + " left in the budget");
+    StreamSlot& s = b->slots[k];
+    s.width = width;
+    s.height = height;
+    s.g = g;
+    s.frame = 0;
+    s.own_inputs = own_inputs != 0;
+    const size_t px = (size_t)width * height;
+    const size_t hist = px * 3 * (b->p.half_history ? 2 : 4);
+    bool ok = true;
+    auto alloc = [&](size_t n, auto** ptr) {
+        if (!ok) return;
+        void* p = nullptr;
+        if (cudaMalloc(&p, n) != cudaSuccess) {
+            cudaGetLastError();
+            ok = false;
+            return;
+        }
+        cudaMemset(p, 0, n);
+        s.allocs.push_back(p);
+        *ptr = static_cast<std::remove_pointer_t<decltype(ptr)>>(p);
+    };
+    for (int i = 0; i < 2; ++i) {
+        alloc(hist, &s.noisy_acc[i]);
+        alloc(hist, &s.acc_filt[i]);
+        alloc(hist, &s.result[i]);
+        alloc(px, &s.spp[i]);
+    }
+    alloc(px * 8, &s.prev_pix);
+    alloc(px, &s.accept);
+    alloc(px * 12, &s.tone_mapped);
+    alloc(px * 12, &s.result_f32);
+    alloc((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &s.weights);
+    alloc((size_t)g.blocks * bmfr::kScaled * 2 * 4, &s.mins_maxs);
+    alloc(bmfr::kNoiseTableBytes, &s.noise);
+    if (s.own_inputs) {
+        for (int i = 0; i < 2; ++i) {
+            alloc(px * 12, &s.normals[i]);
+            alloc(px * 12, &s.positions[i]);
+        }
+        alloc(px * 12, &s.albedo);
+        alloc(px * 12, &s.noisy);
+    }
+    s.bytes = bytes;
+    s.used = true;
+    b->used += bytes;
+    if (!ok) {
+        free_slot(b, s);
+        return fail(BMFR_E_NOMEM, "device allocation for the stream failed");
+    }
+    *slot = k;
+    return BMFR_OK;
+}
+
+int bmfr_batch_remove_stream(bmfr_batch* b, int slot) {
+    if (int st = check_batch(b)) return st;
+    if (int st = check_slot(b, slot)) return st;
+    for (cudaEvent_t e : b->done)   // no step may still use its buffers
+        if (e) cudaEventSynchronize(e);
+    free_slot(b, b->slots[slot]);
+    return BMFR_OK;
+}
+
+int bmfr_batch_reset_stream(bmfr_batch* b, int slot) {
+    if (!b) return fail(BMFR_E_INVALID, "batch is NULL");
+    if (int st = check_slot(b, slot)) return st;
+    b->slots[slot].frame = 0;
+    return BMFR_OK;
+}
+
+int bmfr_batch_stream_frame(const bmfr_batch* b, int slot) {
+    if (!b) return fail(BMFR_E_INVALID, "batch is NULL");
+    if (int st = check_slot(b, slot)) return st;
+    return b->slots[slot].frame;
+}
+
+size_t bmfr_batch_bytes_in_use(const bmfr_batch* b) { return b ? b->used : 0; }
+
+int bmfr_batch_stream_inputs(bmfr_batch* b, int slot, bmfr_frame_inputs* in) {
+    if (!b || !in) return fail(BMFR_E_INVALID, "NULL argument");
+    if (int st = check_slot(b, slot)) return st;
+    StreamSlot& s = b->slots[slot];
+    if (!s.own_inputs) return fail(BMFR_E_STATE, "stream was added without input slots");
+    const int cur = s.frame & 1;
+    in->albedo = s.albedo;
+    in->normals = s.normals[cur];
+    in->positions = s.positions[cur];
+    in->noisy = s.noisy;
+    return BMFR_OK;
+}
+
+int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io* io, const float* matrices,
+                    const float* offsets, void* stream) {
+    if (int st = check_batch(b)) return st;
+    if (n <= 0 || n > BMFR_BATCH_MAX_STREAMS || !slots || !matrices || !offsets)
+        return fail(BMFR_E_INVALID, "step: bad stream list");
+    for (int i = 0; i < n; ++i) {
+        if (int st = check_slot(b, slots[i])) return st;
+        for (int j = 0; j < i; ++j)
+            if (slots[j] == slots[i]) return fail(BMFR_E_INVALID, "step: a stream is listed twice");
+    }
+    if (!b->graphs_valid)
+        if (int st = build_graphs(b)) return st;
+    const int k = b->next;
+    cudaError_t e = cudaEventSynchronize(b->done[k]);   // description buffer k is free again
+    if (e != cudaSuccess) return cuda_fail(e, "step: waiting for an earlier step");
+    if (int st = fill_desc(b, b->h_desc[k], n, slots, io, matrices, offsets)) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->last >= 0) {
+        e = cudaStreamWaitEvent(s, b->done[b->last], 0);
+        if (e != cudaSuccess) return cuda_fail(e, "step: ordering after the previous step");
+    }
+    e = cudaGraphLaunch(b->graph[k], s);
+    if (e == cudaSuccess) e = cudaEventRecord(b->done[k], s);
+    if (e != cudaSuccess) return cuda_fail(e, "step: graph launch");
+    b->last = k;
+    b->next = k ^ 1;
+    for (int i = 0; i < n; ++i) b->slots[slots[i]].frame += 1;
+    return BMFR_OK;
+}
+
+int bmfr_batch_stream_result(const bmfr_batch* b, int slot, const float** result) {
+    if (!b || !result) return fail(BMFR_E_INVALID, "NULL argument");
+    if (int st = check_slot(b, slot)) return st;
+    *result = b->slots[slot].result_f32;
+    return BMFR_OK;
+}
+
+int bmfr_batch_get_tuning(const bmfr_batch* b, bmfr_batch_tuning* t) {
+    if (!b || !t) return fail(BMFR_E_INVALID, "NULL argument");
+    t->block_ctas_per_sm = b->tuning.block_ctas_per_sm;
+    t->taa_tile_w = b->tuning.tile_w;
+    t->taa_tile_h = b->tuning.tile_h;
+    t->staging_depth = b->tuning.staging_depth;
+    return BMFR_OK;
+}
+
+int bmfr_batch_set_tuning(bmfr_batch* b, const bmfr_batch_tuning* t) {
+    if (int st = check_batch(b)) return st;
+    if (!t) return fail(BMFR_E_INVALID, "tuning is NULL");
+    const bool shape_ok = (t->taa_tile_w == 32 && (t->taa_tile_h == 8 || t->taa_tile_h == 4)) ||
+                          (t->taa_tile_w == 64 && t->taa_tile_h == 4) ||
+                          (t->taa_tile_w == 16 && t->taa_tile_h == 16);
+    if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 32x8, 32x4, 64x4 or 16x16");
+    if (t->block_ctas_per_sm < 0 || t->staging_depth < 0 || t->staging_depth > 4)
+        return fail(BMFR_E_INVALID, "bad block CTAs per SM or staging depth");
+    b->tuning.block_ctas_per_sm = t->block_ctas_per_sm;
+    b->tuning.tile_w = t->taa_tile_w;
+    b->tuning.tile_h = t->taa_tile_h;
+    b->tuning.staging_depth = t->staging_depth;
+    return build_graphs(b);
+}
+
+int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io* io, const float* matrices,
+                        const float* offsets, int steps, void* stream, bmfr_batch_tuning* chosen, float* best_ms) {
+    if (int st = check_batch(b)) return st;
+    if (steps < 1) return fail(BMFR_E_INVALID, "autotune needs at least one step");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    auto time_tuning = [&](const bmfr_batch_tuning& t, float* ms) -> int {
+        if (int st = bmfr_batch_set_tuning(b, &t)) return st;
+        if (int st = bmfr_batch_step(b, n, slots, io, matrices, offsets, stream)) return st;   // warm-up
+        cudaEventRecord(t0, s);
+        for (int i = 0; i < steps; ++i)
+            if (int st = bmfr_batch_step(b, n, slots, io, matrices, offsets, stream)) return st;
+        cudaEventRecord(t1, s);
+        cudaError_t e = cudaEventSynchronize(t1);
+        if (e != cudaSuccess) return cuda_fail(e, "autotune timing");
+        cudaEventElapsedTime(ms, t0, t1);
+        *ms /= steps;
+        return BMFR_OK;
+    };
+    bmfr_batch_tuning best{0, 32, 8, 0};
+    float best_t = 1e30f;
+    int status = BMFR_OK;
+    // Blocks per SM and staging depth together, then the TAA CTA shape.
+    for (int ctas = 1; ctas <= b->block_occupancy && status == BMFR_OK; ++ctas) {
+        for (int depth = 0; depth <= 2 && status == BMFR_OK; ++depth) {
+            bmfr_batch_tuning t{ctas, 32, 8, depth};
+            float ms = 0.f;
+            status = time_tuning(t, &ms);
+            if (status == BMFR_OK && ms < best_t) {
+                best_t = ms;
+                best = t;
+            }
+        }
+    }
+    const int shapes[3][2] = {{32, 4}, {64, 4}, {16, 16}};
+    for (int i = 0; i < 3 && status == BMFR_OK; ++i) {
+        bmfr_batch_tuning t = best;
+        t.taa_tile_w = shapes[i][0];
+        t.taa_tile_h = shapes[i][1];
+        float ms = 0.f;
+        status = time_tuning(t, &ms);
+        if (status == BMFR_OK && ms < best_t) {
+            best_t = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (status != BMFR_OK) return status;
+    if (int st = bmfr_batch_set_tuning(b, &best)) return st;
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = best_t;
+    return BMFR_OK;
+}
+
+}  // extern "C"

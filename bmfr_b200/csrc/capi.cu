@@ -6,6 +6,7 @@
 // after every frame and eight single buffers, all resident in HBM.
 #include "bmfr_b200.h"
 #include "kernels.h"
+#include "status.h"
 
 #include <cstdio>
 #include <cstring>
@@ -13,8 +14,10 @@
 #include <vector>
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace bmfr {
 
 int fail(int status, const std::string& msg) {
     g_last_error = msg;
@@ -25,7 +28,10 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(BMFR_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-}  // namespace
+}  // namespace bmfr
+
+using bmfr::cuda_fail;
+using bmfr::fail;
 
 struct bmfr_plan {
     bmfr_params p;

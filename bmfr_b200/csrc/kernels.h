@@ -68,6 +68,15 @@ struct FusedBuffers {
     const float* noise;   // the frame's noise table (launch_noise_table)
 };
 
+// Everything one 32x32 block of one stream needs in the fused block kernel.
+struct BlockJob {
+    Geometry g;
+    AccumArgs a;
+    NoiseConst nc;
+    float second_alpha;
+    FusedBuffers fb;
+};
+
 cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
                                bool fp32_qr, bool half_history, const FusedBuffers& fb, cudaStream_t s);
 

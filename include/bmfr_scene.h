@@ -57,6 +57,15 @@ int bmfr_scene_render(const bmfr_scene_desc* desc, int frame, float* albedo,
                       float* normals, float* positions, float* noisy, float* clean,
                       int threads);
 
+/* The same frame rendered on the current CUDA device into DEVICE buffers:
+ * same scene, camera and noise model as bmfr_scene_render in float
+ * arithmetic, so values agree to float rounding away from object
+ * silhouettes, where a grazing ray may hit a different object.
+ * Asynchronous on `stream` (a cudaStream_t).  At most 64 spheres. */
+int bmfr_scene_render_device(const bmfr_scene_desc* desc, int frame, float* albedo,
+                             float* normals, float* positions, float* noisy, float* clean,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

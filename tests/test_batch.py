@@ -1,0 +1,106 @@
+"""The many-stream engine (include/bmfr_batch.h): every stream's output in a
+batch step must equal what a plan with the same parameters (fused
+pipeline) produces for that stream alone — bit for bit, since both run the
+same block body — whatever other streams share the step."""
+import numpy as np
+import pytest
+
+import bmfr_b200 as B
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(96, 64), (160, 96), (128, 128), (200, 120)]
+
+
+class Stream:
+    """One render stream: its scene, device frames and a reference plan."""
+
+    def __init__(self, k, w, h, params, dev):
+        import torch
+        self.w, self.h = w, h
+        self.sc = B.Scene(100 + k, w, h, 8 + 4 * k, orbit_degrees_per_frame=0.3 + 0.2 * k)
+        self.frames = []
+        self.dev = dev
+        self.plan = B.Plan(w, h, params=params)
+        self.torch = torch
+
+    def frame(self, f):
+        while len(self.frames) <= f:
+            d = self.sc.render(len(self.frames))
+            self.frames.append({k: self.torch.from_numpy(v).to(self.dev) for k, v in d.items()})
+        return self.frames[f]
+
+    def io(self, f):
+        d, p = self.frame(f), self.frame(max(f - 1, 0))
+        return B.Batch.frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"], p["positions"])
+
+    def plan_step(self, f):
+        d, p = self.frame(f), self.frame(max(f - 1, 0))
+        out = self.torch.empty(self.w * self.h * 3, dtype=self.torch.float32, device=self.dev)
+        self.plan.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"],
+                                   p["positions"], self.sc.prev_camera(f), self.sc.pixel_offset(f), result=out)
+        return out
+
+
+def _device_result(ptr, w, h):
+    import torch
+    from test_parity_pipeline import device_array
+    return device_array(ptr, (h, w, 3), np.float32)
+
+
+@pytest.mark.parametrize("precision_form", [True, False])
+def test_batch_equals_streams_alone(cuda, precision_form):
+    import torch
+    kw = dict(fp32_qr=1, half_history=1) if precision_form else {}
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, **kw)
+    streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
+    batch = B.Batch(params)
+    slots = [batch.add_stream(s.w, s.h) for s in streams]
+    # Step schedule: all, a subset (stream 1 and 3 idle), all, all.
+    schedule = [[0, 1, 2, 3], [0, 2], [0, 1, 2, 3], [3, 1, 0, 2]]
+    frame = [0] * len(streams)
+    for active in schedule:
+        io = [streams[i].io(frame[i]) for i in active]
+        mats = np.concatenate([streams[i].sc.prev_camera(frame[i]) for i in active])
+        offs = np.concatenate([streams[i].sc.pixel_offset(frame[i]) for i in active])
+        batch.step([slots[i] for i in active], mats, offs, io=io)
+        for i in active:
+            want = streams[i].plan_step(frame[i]).cpu().numpy().reshape(streams[i].h, streams[i].w, 3)
+            got = _device_result(batch.result_ptr(slots[i]), streams[i].w, streams[i].h)
+            np.testing.assert_array_equal(got, want, err_msg=f"stream {i} frame {frame[i]}")
+            frame[i] += 1
+            assert batch.frame(slots[i]) == frame[i]
+    torch.cuda.synchronize()
+    batch.close()
+
+
+def test_batch_autotune_and_budget(cuda):
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES[:3])]
+    batch = B.Batch(params)
+    slots = [batch.add_stream(s.w, s.h) for s in streams]
+    io = [s.io(0) for s in streams]
+    mats = np.concatenate([s.sc.prev_camera(0) for s in streams])
+    offs = np.concatenate([s.sc.pixel_offset(0) for s in streams])
+    t, ms = batch.autotune(slots, mats, offs, io=io, steps=1)
+    assert ms > 0 and (t.taa_tile_w, t.taa_tile_h) in [(32, 8), (32, 4), (64, 4), (16, 16)]
+    assert 0 <= t.staging_depth <= 2 and t.block_ctas_per_sm >= 1
+    # After tuning, a reset stream starts over and still matches its plan.
+    for s_, sl in zip(streams, slots):
+        batch.reset_stream(sl)
+    batch.step(slots, mats, offs, io=io)
+    for s_, sl in zip(streams, slots):
+        want = s_.plan_step(0).cpu().numpy().reshape(s_.h, s_.w, 3)
+        np.testing.assert_array_equal(_device_result(batch.result_ptr(sl), s_.w, s_.h), want)
+    batch.close()
+
+    need = B.Batch.stream_bytes(params, 200, 120)
+    small = B.Batch(params, memory_budget_bytes=need + need // 2)
+    small.add_stream(200, 120)
+    with pytest.raises(B.BmfrError) as e:
+        small.add_stream(200, 120)
+    assert e.value.status == B._native.BMFR_E_BUDGET
+    assert small.bytes_in_use == need
+    small.close()
+    torch.cuda.synchronize()
