@@ -189,6 +189,124 @@ def run_reference(args, world, rank):
     }), flush=True)
 
 
+BATCH_STREAMS = [(640, 360)] * 8 + [(1280, 720)] * 8 + [(1920, 1080)] * 6 + [(3840, 2160)] * 2
+BATCH_FRAMES = 30
+
+
+def batch_scenes(rank):
+    """The batched form's 24 streams: own seed, U{8..32} spheres, U[0.2,1.0] deg/frame."""
+    import bmfr_b200 as B
+    rng = np.random.default_rng(SEED + 17 + rank)
+    return [B.Scene(SEED + 1000 * rank + k, w, h, int(rng.integers(8, 33)),
+                    orbit_degrees_per_frame=float(rng.uniform(0.2, 1.0)))
+            for k, (w, h) in enumerate(BATCH_STREAMS)]
+
+
+def run_batched(args, world, rank, local, dev, barrier, pg):
+    """Batched form: 24 streams of uneven size, one graph-captured step per
+    frame of every stream, binary16 histories and FP32 QR, autotuned; next to
+    the plain per-frame path on the same streams."""
+    import torch
+    import bmfr_b200 as B
+    scenes = batch_scenes(rank)
+    nfr = max(2, min(args.frames, BATCH_FRAMES))
+    stream = torch.cuda.Stream(device=dev)
+    frames = []
+    for sc in scenes:
+        px = sc.width * sc.height * 3
+        fl = []
+        for f in range(nfr):
+            d = {k: torch.empty(px, dtype=torch.float32, device=dev) for k in ("albedo", "normals", "positions", "noisy")}
+            sc.render_device(f, d["albedo"], d["normals"], d["positions"], d["noisy"], stream=stream)
+            fl.append(d)
+        frames.append(fl)
+    stream.synchronize()
+    n = len(scenes)
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    batch = B.Batch(params)
+    slots = [batch.add_stream(sc.width, sc.height) for sc in scenes]
+
+    def step_args(i):
+        f = frame_order(i, nfr)
+        pf = frame_order(i - 1, nfr) if i > 0 else f
+        io = []
+        for k in range(n):
+            d, p = frames[k][f], frames[k][pf]
+            io.append(B.Batch.frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"],
+                                       p["positions"]))
+        mats = np.concatenate([sc.camera(pf) for sc in scenes])
+        offs = np.concatenate([sc.pixel_offset(f) for sc in scenes])
+        return io, mats, offs
+
+    io0, m0, o0 = step_args(0)
+    tuning, tuned_ms = batch.autotune(slots, m0, o0, io=io0, steps=2, stream=stream)
+    for sl in slots:
+        batch.reset_stream(sl)
+    for i in range(args.warmup):
+        io, m, o = step_args(i)
+        batch.step(slots, m, o, io=io, stream=stream)
+    stream.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for i in range(args.warmup, args.warmup + args.steps):
+            io, m, o = step_args(i)
+            batch.step(slots, m, o, io=io, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * args.steps / (ms / 1e3)
+    batch.close()
+
+    # The plain path (reference arithmetic, float histories, staged pipeline)
+    # on the same streams, one frame at a time.
+    plans = [B.Plan(sc.width, sc.height, position_limit_squared=sc.position_limit_squared,
+                    normal_limit_squared=sc.normal_limit_squared) for sc in scenes]
+    plain_steps = min(args.steps, 10)
+
+    def plain_step(i):
+        f = frame_order(i, nfr)
+        pf = frame_order(i - 1, nfr) if i > 0 else f
+        for k, (sc, pl) in enumerate(zip(scenes, plans)):
+            d, p = frames[k][f], frames[k][pf]
+            pl.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"], p["positions"],
+                                sc.camera(pf), sc.pixel_offset(f), stream=stream)
+
+    for i in range(3):
+        plain_step(i)
+    stream.synchronize()
+    e0.record(stream)
+    for i in range(3, 3 + plain_steps):
+        plain_step(i)
+    e1.record(stream)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_value = n * plain_steps / (plain_ms / 1e3)
+    for pl in plans:
+        pl.close()
+    pixels = sum(w * h for w, h in BATCH_STREAMS)
+    if rank == 0:
+        print(json.dumps({
+            "form": "batched", "metric": "multi-stream frames/s (24 streams: 8x640x360, 8x1280x720, 6x1920x1080, 2x3840x2160)",
+            "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered, 30 frames per stream)",
+            "config": {"workload": "batched form, 24 streams", "streams": len(BATCH_STREAMS),
+                       "pixels_per_step": pixels, "frames": nfr, "tuning": {
+                           "block_ctas_per_sm": tuning.block_ctas_per_sm, "taa_tile": [tuning.taa_tile_w, tuning.taa_tile_h],
+                           "staging_depth": tuning.staging_depth}, "tuned_ms_per_step": tuned_ms},
+            "plain_path": {"value": plain_value, "unit": "frames/s", "ms_per_round": plain_ms / plain_steps,
+                           "how": "one plan per stream, staged pipeline, reference arithmetic, frames in turn"},
+            "speedup_vs_plain": value / plain_value / world,
+            "clocks": clocks.summary(), "gpu_launches": 3 * args.steps,
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,6 +316,7 @@ def main():
     ap.add_argument("--pipeline", default="staged", choices=["fused", "staged"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=FRAMES, help="distinct scene frames held in HBM")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "precision"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -221,6 +340,12 @@ def main():
     def barrier():
         if pg is not None:
             pg.barrier()
+
+    if args.form == "batched":
+        run_batched(args, world, rank, local, dev, barrier, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     # Inputs: every rank denoises its own stream (replicas).
     nfr = max(2, min(args.frames, FRAMES))

@@ -42,13 +42,14 @@
 namespace bmfr {
 
 struct FitterSmem {
-    float part[12 * 64];   // first-stage partial sums, 64 per batched value
-    float out[12];         // reduction results
+    float part[13 * 64];   // first-stage partial sums, 64 per batched value
+    float out[16];         // reduction results
     float ucl;             // u[col] broadcast from its owner
     int status;            // nonzero: a bounded wait ran out
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
-    float part2[12 * 8];   // second-stage sums, 8 per batched value
+    float part2[13 * 8];   // second-stage sums, 8 per batched value
+    float rowc[13];        // the precision form: row `col` of every column
 };
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -160,18 +161,21 @@ struct Tile<true> {   // binary16 storage: every store rounds to nearest even
 };
 
 template <>
-struct Tile<false> {   // float storage: no intermediate rounding
-    float f[kBuffers][4];
-    __device__ __forceinline__ float2 get2(int k, int p) const { return make_float2(f[k][2 * p], f[k][2 * p + 1]); }
-    __device__ __forceinline__ void set2(int k, int p, float a, float b) {
-        f[k][2 * p] = a;
-        f[k][2 * p + 1] = b;
+struct Tile<false> {   // float storage: no intermediate rounding; rows (q0,q1) and (q2,q3) paired
+    float2 p[kBuffers][2];
+    __device__ __forceinline__ float2 get2(int k, int h) const { return p[k][h]; }
+    __device__ __forceinline__ void set2(int k, int h, float a, float b) { p[k][h] = make_float2(a, b); }
+    __device__ __forceinline__ float get1(int k, int q) const { return (q & 1) ? p[k][q >> 1].y : p[k][q >> 1].x; }
+    __device__ __forceinline__ void set1(int k, int q, float v) {
+        if (q & 1) p[k][q >> 1].y = v;
+        else p[k][q >> 1].x = v;
     }
     __device__ __forceinline__ void shift() {
 #pragma unroll
-        for (int k = 0; k < kBuffers - 1; ++k)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) f[k][q] = f[k + 1][q];
+        for (int k = 0; k < kBuffers - 1; ++k) {
+            p[k][0] = p[k + 1][0];
+            p[k][1] = p[k + 1][1];
+        }
     }
 };
 
@@ -357,85 +361,128 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     t.shift();
 }
 
-// The precision form's column (FP32 QR): the same reflections and reduction
-// trees with the block kept in float, fused multiply-adds in the dot
-// products and updates, and the update written as a - u * (2 dot / |u|^2).
-// It no longer rounds like the reference; it is checked against the fp64
-// fitter instead.
-template <bool NOISE>
-__device__ __forceinline__ void qr_column_fast(Tile<false>& t, int col, int id, const float* __restrict__ noise,
-                                               NoiseConst nc, FitterSmem& sm) {
-    const int V = kBuffers - 1 - col;
-    const float c0 = t.f[0][0], c1 = t.f[0][1], c2 = t.f[0][2], c3 = t.f[0][3];
-    float nv[1];
+// The precision form's fit (FP32 QR).  The same Householder reflections in
+// float with fused multiply-adds, and one batched reduction per column
+// instead of two: because the reflection vector u differs from the column
+// itself only in row `col`, every dot product u . a_j equals
+// sum_{i>=col} a_col[i] a_j[i] - vl * a_j[col], so the norm and all Gram
+// sums of a column are reduced together, and each column's partial sums are
+// formed right after the previous column's update.  All packed arithmetic
+// pairs rows (q0,q1) and (q2,q3), the tile's register pairs.  It rounds
+// differently from the reference and is checked against the fp64 fitter.
+
+// Sum over the CTA of v[0..15] (any order); result k in sm.out[k].  A
+// transposing butterfly leaves each lane pair with one value summed over
+// the warp; eight warps then meet in shared memory.
+__device__ __forceinline__ void block_sum16(float (&v)[16], FitterSmem& sm) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const bool up = lane & 16;
+        const float send = up ? v[k] : v[k + 8], keep = up ? v[k + 8] : v[k];
+        v[k] = keep + __shfl_xor_sync(kFull, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const bool up = lane & 8;
+        const float send = up ? v[k] : v[k + 4], keep = up ? v[k + 4] : v[k];
+        v[k] = keep + __shfl_xor_sync(kFull, send, 8);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool up = lane & 4;
+        const float send = up ? v[k] : v[k + 2], keep = up ? v[k + 2] : v[k];
+        v[k] = keep + __shfl_xor_sync(kFull, send, 4);
+    }
     {
-        float s = (id >= col + 1) ? c0 * c0 : 0.0f;
-        s = __fmaf_rn(c1, c1, s);
-        s = __fmaf_rn(c2, c2, s);
-        s = __fmaf_rn(c3, c3, s);
-        nv[0] = s;
+        const bool up = lane & 2;
+        const float send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(kFull, send, 2);
     }
-    if (id == col) sm.ucl = c0;
-    block_reduce<1, 0, 0>(nv, 1, 1, sm);
-    const float norm2 = sm.out[0];
-    const float ucl = sm.ucl;
-    const float vl = sqrtf(__fmaf_rn(ucl, ucl, norm2));
-    const float ucl_new = ucl - vl;
-    const float uls = __fmaf_rn(ucl_new, ucl_new, norm2);
-    if (id < col) sm.Rm[col][id] = c0;
-    if (id == col) sm.Rm[col][col] = vl;
-    const bool row0 = id >= col;
-    const float u0 = id == col ? ucl_new : c0;
-    const float2 uq0 = dup2(row0 ? u0 : 0.0f), uq1 = dup2(c1), uq2 = dup2(c2), uq3 = dup2(c3);
-    const float2 hi = dup2(nc.hi);
-    auto column = [&](int k, float2& a01, float2& a23) {
-        a01 = make_float2(t.f[k][0], t.f[k][1]);
-        a23 = make_float2(t.f[k][2], t.f[k][3]);
-        if (NOISE && k < kFeatures) {
-            const float* r = noise + (k - 1) * 4 * kLocal + threadIdx.x;
-            a01 = fma2(hi, make_float2(r[0], r[kLocal]), a01);
-            a23 = fma2(hi, make_float2(r[2 * kLocal], r[3 * kLocal]), a23);
-        }
-    };
-    float d[12];
-#pragma unroll
-    for (int i = 0; i < 12; i += 2) {
-        d[i] = d[i + 1] = 0.0f;
-        if (i < V) {
-            float2 a01, a23, b01, b23;
-            column(i + 1, a01, a23);
-            column(i + 2, b01, b23);
-            float2 sacc = mul2(make_float2(a01.x, b01.x), uq0);
-            sacc = fma2(make_float2(a01.y, b01.y), uq1, sacc);
-            sacc = fma2(make_float2(a23.x, b23.x), uq2, sacc);
-            sacc = fma2(make_float2(a23.y, b23.y), uq3, sacc);
-            d[i] = sacc.x;
-            d[i + 1] = sacc.y;
-        }
+    v[0] = v[0] + __shfl_xor_sync(kFull, v[0], 1);
+    const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+    if ((lane & 1) == 0) sm.part[idx * 8 + warp] = v[0];
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        const float* p = sm.part + threadIdx.x * 8;
+        sm.out[threadIdx.x] = ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
     }
-    block_reduce<12, 0, 0>(d, V, V, sm);
-    const float y2 = 2.0f * __frcp_rn(uls);
-    const float2 nu01 = make_float2(row0 ? -u0 : 0.0f, -c1), nu23 = make_float2(-c2, -c3);
-#pragma unroll
-    for (int i = 0; i < 12; ++i) {
-        if (i < V) {
-            const float2 w = dup2(sm.out[i] * y2);
-            float2 a01, a23;
-            column(i + 1, a01, a23);
-            a01 = fma2(nu01, w, a01);
-            a23 = fma2(nu23, w, a23);
-            t.f[i + 1][0] = a01.x;
-            t.f[i + 1][1] = a01.y;
-            t.f[i + 1][2] = a23.x;
-            t.f[i + 1][3] = a23.y;
-        }
-    }
-    t.shift();
+    __syncthreads();
 }
 
-// Fits one block held in t (the values as loaded from tmp_data) and writes
-// its 30 weights and 12 min/max values.  Ends with a barrier.
-// FAST (float tile only): the precision form's FP32 QR (qr_column_fast).
+// Partial sums of column `col` (tile column 0): v[0] the norm of rows
+// >= col+1, v[1+i] the Gram sum of rows >= col with tile column 1+i.
+__device__ __forceinline__ void fast_partials(const Tile<false>& t, int col, int id, FitterSmem& sm,
+                                              float (&v)[16]) {
+    const int V = kBuffers - 1 - col;
+    const float2 c01 = t.p[0][0], c23 = t.p[0][1];
+    const float2 cn = make_float2(id >= col + 1 ? c01.x : 0.0f, c01.y);
+    const float2 cg = make_float2(id >= col ? c01.x : 0.0f, c01.y);
+    float2 n = fma2(c23, c23, mul2(cn, cn));
+    v[0] = n.x + n.y;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        v[1 + i] = 0.0f;
+        if (i < V) {
+            const float2 g = fma2(t.p[i + 1][1], c23, mul2(t.p[i + 1][0], cg));
+            v[1 + i] = g.x + g.y;
+        }
+    }
+    v[13] = v[14] = v[15] = 0.0f;
+    if (id == col) {   // row `col` of every column, for the dot products and u
+#pragma unroll
+        for (int k = 0; k < kBuffers; ++k)
+            if (k <= V) sm.rowc[k] = t.p[k][0].x;
+    }
+}
+
+__device__ __forceinline__ void fit_columns_fast(Tile<false>& t, int id, const float* __restrict__ noise,
+                                                 NoiseConst nc, FitterSmem& sm) {
+    // The noise of features 1..9 (bmfr.cl:625-627) goes in before the first
+    // column's sums; in the reference it enters at the first load and stays.
+    const float2 hi = dup2(nc.hi);
+#pragma unroll
+    for (int k = 1; k < kFeatures; ++k) {
+        const float* r = noise + (k - 1) * 4 * kLocal + threadIdx.x;
+        t.p[k][0] = fma2(hi, make_float2(r[0], r[kLocal]), t.p[k][0]);
+        t.p[k][1] = fma2(hi, make_float2(r[2 * kLocal], r[3 * kLocal]), t.p[k][1]);
+    }
+    float v[16];
+    fast_partials(t, 0, id, sm, v);
+#pragma unroll 1
+    for (int col = 0; col < kFeatures; ++col) {
+        const int V = kBuffers - 1 - col;
+        block_sum16(v, sm);
+        const float norm2 = sm.out[0];
+        const float ucl = sm.rowc[0];
+        const float vl = sqrtf(__fmaf_rn(ucl, ucl, norm2));
+        const float ucl_new = ucl - vl;
+        const float uls = __fmaf_rn(ucl_new, ucl_new, norm2);
+        const float2 c01 = t.p[0][0], c23 = t.p[0][1];
+        if (id < col) sm.Rm[col][id] = c01.x;
+        if (id == col) sm.Rm[col][col] = vl;
+        const bool row0 = id >= col;
+        const float u0 = id == col ? ucl_new : c01.x;
+        const float2 nu01 = make_float2(row0 ? -u0 : 0.0f, -c01.y), nu23 = make_float2(-c23.x, -c23.y);
+        const float y2 = 2.0f * __frcp_rn(uls);
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+            if (i < V) {
+                const float dot = __fmaf_rn(-sm.rowc[i + 1], vl, sm.out[i + 1]);   // u . a_j
+                const float2 w = dup2(dot * y2);
+                t.p[i + 1][0] = fma2(nu01, w, t.p[i + 1][0]);
+                t.p[i + 1][1] = fma2(nu23, w, t.p[i + 1][1]);
+            }
+        }
+        t.shift();
+        if (col + 1 < kFeatures) {
+            __syncthreads();   // rowc of this column is read; the next owner may write it
+            fast_partials(t, col + 1, id, sm, v);
+        }
+    }
+}
+
+// FAST (float tile only): the precision form's FP32 QR (fit_columns_fast).
 template <bool HALF, bool FAST = false>
 __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict__ noise, NoiseConst nc,
                                           FitterSmem& sm, float* __restrict__ weights_out,
@@ -470,9 +517,7 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
     }
 
     if constexpr (FAST && !HALF) {
-        qr_column_fast<true>(t, 0, id, noise, nc, sm);
-#pragma unroll 1
-        for (int col = 1; col < kFeatures; ++col) qr_column_fast<false>(t, col, id, noise, nc, sm);
+        fit_columns_fast(t, id, noise, nc, sm);
     } else {
         qr_column<HALF, true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1

@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    if constexpr (HALF_TMP) t.f[k][q] = __half2float(col[q * kLocal]);
-                    else t.f[k][q] = col[q * kLocal];
+                    if constexpr (HALF_TMP) t.set1(k, q, __half2float(col[q * kLocal]));
+                    else t.set1(k, q, col[q * kLocal]);
                 }
             }
         }

@@ -20,7 +20,7 @@ __device__ __forceinline__ void tile_set1(Tile<true>& t, int k, int q, float v) 
 }
 template <>
 __device__ __forceinline__ void tile_set1(Tile<false>& t, int k, int q, float v) {
-    t.f[k][q] = v;
+    t.set1(k, q, v);
 }
 
 // ROUND: binary16 tile rounded at every store (reference arithmetic);
