@@ -410,31 +410,63 @@ __device__ __forceinline__ void block_sum16(float (&v)[16], FitterSmem& sm) {
     __syncthreads();
 }
 
-// Partial sums of column `col` (tile column 0): v[0] the norm of rows
-// >= col+1, v[1+i] the Gram sum of rows >= col with tile column 1+i.
-__device__ __forceinline__ void fast_partials(const Tile<false>& t, int col, int id, FitterSmem& sm,
-                                              float (&v)[16]) {
-    const int V = kBuffers - 1 - col;
-    const float2 c01 = t.p[0][0], c23 = t.p[0][1];
-    const float2 cn = make_float2(id >= col + 1 ? c01.x : 0.0f, c01.y);
-    const float2 cg = make_float2(id >= col ? c01.x : 0.0f, c01.y);
-    float2 n = fma2(c23, c23, mul2(cn, cn));
+// Partial sums of column COL, held in tile column COL: v[0] the norm of
+// rows >= COL+1, v[1+i] the Gram sum of rows >= COL with column COL+1+i.
+// The column loop is unrolled, so every tile index is a constant.
+template <int COL>
+__device__ __forceinline__ void fast_partials(const Tile<false>& t, int id, FitterSmem& sm, float (&v)[16]) {
+    constexpr int V = kBuffers - 1 - COL;
+    const float2 c01 = t.p[COL][0], c23 = t.p[COL][1];
+    const float2 cn = make_float2(id >= COL + 1 ? c01.x : 0.0f, c01.y);
+    const float2 cg = make_float2(id >= COL ? c01.x : 0.0f, c01.y);
+    const float2 n = fma2(c23, c23, mul2(cn, cn));
     v[0] = n.x + n.y;
 #pragma unroll
-    for (int i = 0; i < 12; ++i) {
-        v[1 + i] = 0.0f;
+    for (int i = 0; i < 15; ++i) {
         if (i < V) {
-            const float2 g = fma2(t.p[i + 1][1], c23, mul2(t.p[i + 1][0], cg));
+            const float2 g = fma2(t.p[COL + 1 + i][1], c23, mul2(t.p[COL + 1 + i][0], cg));
             v[1 + i] = g.x + g.y;
+        } else {
+            v[1 + i] = 0.0f;
         }
     }
-    v[13] = v[14] = v[15] = 0.0f;
-    if (id == col) {   // row `col` of every column, for the dot products and u
+    if (id == COL) {   // row COL of every column, for the dot products and u
 #pragma unroll
-        for (int k = 0; k < kBuffers; ++k)
-            if (k <= V) sm.rowc[k] = t.p[k][0].x;
+        for (int k = COL; k < kBuffers; ++k) sm.rowc[k - COL] = t.p[k][0].x;
     }
 }
+
+template <int COL>
+struct FastColumn {
+    static __device__ __forceinline__ void run(Tile<false>& t, int id, FitterSmem& sm, float (&v)[16]) {
+        constexpr int V = kBuffers - 1 - COL;
+        block_sum16(v, sm);
+        const float norm2 = sm.out[0];
+        const float ucl = sm.rowc[0];
+        const float vl = sqrtf(__fmaf_rn(ucl, ucl, norm2));
+        const float ucl_new = ucl - vl;
+        const float uls = __fmaf_rn(ucl_new, ucl_new, norm2);
+        const float2 c01 = t.p[COL][0], c23 = t.p[COL][1];
+        if (id < COL) sm.Rm[COL][id] = c01.x;
+        if (id == COL) sm.Rm[COL][COL] = vl;
+        const bool row0 = id >= COL;
+        const float u0 = id == COL ? ucl_new : c01.x;
+        const float2 nu01 = make_float2(row0 ? -u0 : 0.0f, -c01.y), nu23 = make_float2(-c23.x, -c23.y);
+        const float y2 = 2.0f * __frcp_rn(uls);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+            const float dot = __fmaf_rn(-sm.rowc[i + 1], vl, sm.out[i + 1]);   // u . a_j
+            const float2 w = dup2(dot * y2);
+            t.p[COL + 1 + i][0] = fma2(nu01, w, t.p[COL + 1 + i][0]);
+            t.p[COL + 1 + i][1] = fma2(nu23, w, t.p[COL + 1 + i][1]);
+        }
+        if constexpr (COL + 1 < kFeatures) {
+            __syncthreads();   // rowc of this column is read; the next owner may write it
+            fast_partials<COL + 1>(t, id, sm, v);
+            FastColumn<COL + 1>::run(t, id, sm, v);
+        }
+    }
+};
 
 __device__ __forceinline__ void fit_columns_fast(Tile<false>& t, int id, const float* __restrict__ noise,
                                                  NoiseConst nc, FitterSmem& sm) {
@@ -448,37 +480,14 @@ __device__ __forceinline__ void fit_columns_fast(Tile<false>& t, int id, const f
         t.p[k][1] = fma2(hi, make_float2(r[2 * kLocal], r[3 * kLocal]), t.p[k][1]);
     }
     float v[16];
-    fast_partials(t, 0, id, sm, v);
-#pragma unroll 1
-    for (int col = 0; col < kFeatures; ++col) {
-        const int V = kBuffers - 1 - col;
-        block_sum16(v, sm);
-        const float norm2 = sm.out[0];
-        const float ucl = sm.rowc[0];
-        const float vl = sqrtf(__fmaf_rn(ucl, ucl, norm2));
-        const float ucl_new = ucl - vl;
-        const float uls = __fmaf_rn(ucl_new, ucl_new, norm2);
-        const float2 c01 = t.p[0][0], c23 = t.p[0][1];
-        if (id < col) sm.Rm[col][id] = c01.x;
-        if (id == col) sm.Rm[col][col] = vl;
-        const bool row0 = id >= col;
-        const float u0 = id == col ? ucl_new : c01.x;
-        const float2 nu01 = make_float2(row0 ? -u0 : 0.0f, -c01.y), nu23 = make_float2(-c23.x, -c23.y);
-        const float y2 = 2.0f * __frcp_rn(uls);
+    fast_partials<0>(t, id, sm, v);
+    FastColumn<0>::run(t, id, sm, v);
+    // The colour columns are tile columns 10..12; move them to 0..2 where
+    // the back substitution reads them.
 #pragma unroll
-        for (int i = 0; i < 12; ++i) {
-            if (i < V) {
-                const float dot = __fmaf_rn(-sm.rowc[i + 1], vl, sm.out[i + 1]);   // u . a_j
-                const float2 w = dup2(dot * y2);
-                t.p[i + 1][0] = fma2(nu01, w, t.p[i + 1][0]);
-                t.p[i + 1][1] = fma2(nu23, w, t.p[i + 1][1]);
-            }
-        }
-        t.shift();
-        if (col + 1 < kFeatures) {
-            __syncthreads();   // rowc of this column is read; the next owner may write it
-            fast_partials(t, col + 1, id, sm, v);
-        }
+    for (int c = 0; c < 3; ++c) {
+        t.p[c][0] = t.p[kFeatures + c][0];
+        t.p[c][1] = t.p[kFeatures + c][1];
     }
 }
 
