@@ -15,11 +15,11 @@ import ctypes as C
 import numpy as np
 
 from . import _native
-from ._native import (BatchTuning, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check,
+from ._native import (BatchTuning, ServerConfig, ServerStats, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check,
                       lib, PIPELINE_FUSED, PIPELINE_STAGED)
 
 __all__ = [
-    "Plan", "Batch", "Scene", "BmfrError", "default_params", "block_offsets",
+    "Plan", "Batch", "Server", "Scene", "BmfrError", "default_params", "block_offsets",
     "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
     "PIPELINE_FUSED", "PIPELINE_STAGED", "library_path",
 ]
@@ -406,6 +406,78 @@ class Batch:
         check(lib.bmfr_batch_autotune(self.handle, n, sl, iop, mp, op, int(steps), _stream_ptr(stream),
                                       C.byref(t), C.byref(ms)), "bmfr_batch_autotune")
         return t, ms.value
+
+
+class Server:
+    """Continuous batching of frame requests from many render streams
+    (include/bmfr_batch.h, bmfr_server_*)."""
+
+    def __init__(self, params: Params | None = None, memory_budget_bytes: int = 0, max_streams_per_step: int = 0,
+                 own_inputs: bool = False, **overrides):
+        self.params = params if params is not None else default_params(pipeline=PIPELINE_FUSED, **overrides)
+        cfg = ServerConfig(int(memory_budget_bytes), int(max_streams_per_step), int(own_inputs))
+        h = C.c_void_p()
+        check(lib.bmfr_server_create(C.byref(self.params), C.byref(cfg), C.byref(h)), "bmfr_server_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise BmfrError(_native.BMFR_E_STATE, "server destroyed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib.bmfr_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def open_stream(self, width: int, height: int) -> int:
+        sid = C.c_int()
+        check(lib.bmfr_server_open_stream(self.handle, int(width), int(height), C.byref(sid)),
+              "bmfr_server_open_stream")
+        return sid.value
+
+    def close_stream(self, sid: int) -> None:
+        check(lib.bmfr_server_close_stream(self.handle, int(sid)), "bmfr_server_close_stream")
+
+    def submit(self, sid: int, matrix, offset, io: FrameIO | None = None) -> int:
+        m, mp = _f32(matrix, 16, "matrix")
+        o, op = _f32(offset, 2, "offset")
+        rid = C.c_uint64()
+        check(lib.bmfr_server_submit(self.handle, int(sid), C.byref(io) if io is not None else None, mp, op,
+                                     C.byref(rid)), "bmfr_server_submit")
+        return rid.value
+
+    def poll(self, rid: int):
+        done, lat = C.c_int(), C.c_double()
+        check(lib.bmfr_server_poll(self.handle, C.c_uint64(rid), C.byref(done), C.byref(lat)), "bmfr_server_poll")
+        return bool(done.value), lat.value
+
+    def drain(self, timeout_ms: float = 60000.0) -> None:
+        check(lib.bmfr_server_drain(self.handle, float(timeout_ms)), "bmfr_server_drain")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib.bmfr_server_stats_get(self.handle, C.byref(st)), "bmfr_server_stats_get")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        check(lib.bmfr_server_stats_reset(self.handle), "bmfr_server_stats_reset")
+
+    def set_tuning(self, t: BatchTuning) -> None:
+        check(lib.bmfr_server_set_tuning(self.handle, C.byref(t)), "bmfr_server_set_tuning")
 
 
 # -- input source ------------------------------------------------------------

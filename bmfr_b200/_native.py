@@ -79,6 +79,20 @@ class BatchTuning(C.Structure):
                 ("staging_depth", C.c_int)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_streams_per_step", C.c_int), ("own_inputs", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_submitted", C.c_uint64), ("requests_completed", C.c_uint64),
+                ("steps", C.c_uint64), ("frames", C.c_uint64),
+                ("streams_admitted", C.c_uint64), ("streams_rejected", C.c_uint64),
+                ("p50_latency_ms", C.c_double), ("p99_latency_ms", C.c_double),
+                ("max_latency_ms", C.c_double), ("mean_latency_ms", C.c_double),
+                ("mean_frames_per_step", C.c_double), ("busy_seconds", C.c_double),
+                ("elapsed_seconds", C.c_double)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("width", C.c_int), ("height", C.c_int),
@@ -140,6 +154,18 @@ def _load() -> C.CDLL:
         "bmfr_batch_set_tuning": (i, [vp, C.POINTER(BatchTuning)]),
         "bmfr_batch_autotune": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, i, vp,
                                     C.POINTER(BatchTuning), C.POINTER(C.c_float)]),
+        "bmfr_server_create": (i, [C.POINTER(Params), C.POINTER(ServerConfig), C.POINTER(vp)]),
+        "bmfr_server_destroy": (i, [vp]),
+        "bmfr_server_open_stream": (i, [vp, i, i, C.POINTER(i)]),
+        "bmfr_server_close_stream": (i, [vp, i]),
+        "bmfr_server_stream_inputs": (i, [vp, i, C.POINTER(FrameInputs)]),
+        "bmfr_server_submit": (i, [vp, i, C.POINTER(FrameIO), fp, fp, C.POINTER(C.c_uint64)]),
+        "bmfr_server_poll": (i, [vp, C.c_uint64, C.POINTER(i), C.POINTER(C.c_double)]),
+        "bmfr_server_drain": (i, [vp, C.c_double]),
+        "bmfr_server_stats_get": (i, [vp, C.POINTER(ServerStats)]),
+        "bmfr_server_stats_reset": (i, [vp]),
+        "bmfr_server_batch": (vp, [vp]),
+        "bmfr_server_set_tuning": (i, [vp, C.POINTER(BatchTuning)]),
         "bmfr_last_error": (C.c_char_p, []),
         "bmfr_status_string": (C.c_char_p, [i]),
         "bmfr_scene_default": (i, [C.POINTER(SceneDesc), C.c_uint64, i, i, i]),

@@ -86,6 +86,60 @@ int bmfr_batch_autotune(bmfr_batch* batch, int n, const int* slots, const bmfr_f
                         const float* matrices, const float* offsets, int steps, void* stream,
                         bmfr_batch_tuning* chosen, float* best_ms);
 
+/* ---- server: continuous batching of frame requests ---------------------- */
+
+typedef struct bmfr_server bmfr_server;
+
+typedef struct bmfr_server_config {
+    size_t memory_budget_bytes;  /* device bytes all streams may hold (0: no limit) */
+    int max_streams_per_step;    /* at most this many frames per step (0: every stream that is ready) */
+    int own_inputs;              /* streams get input slots (bmfr_server_stream_inputs) */
+} bmfr_server_config;
+
+typedef struct bmfr_server_stats {
+    uint64_t requests_submitted, requests_completed;
+    uint64_t steps, frames;
+    uint64_t streams_admitted, streams_rejected;
+    double p50_latency_ms, p99_latency_ms, max_latency_ms, mean_latency_ms;
+    double mean_frames_per_step;
+    double busy_seconds;          /* wall time with at least one step in flight */
+    double elapsed_seconds;       /* since the server started or the stats were reset */
+} bmfr_server_stats;
+
+/* Starts the server's scheduling thread on the current device.  Requests
+ * that arrive while steps are on the GPU are queued and join the next step;
+ * each step takes the oldest pending frame of every ready stream. */
+int bmfr_server_create(const bmfr_params* params, const bmfr_server_config* config, bmfr_server** server);
+int bmfr_server_destroy(bmfr_server* server);   /* finishes queued work first */
+
+/* Admits a render stream if its histories fit in the memory budget
+ * (BMFR_E_BUDGET otherwise; retry once streams close). */
+int bmfr_server_open_stream(bmfr_server* server, int width, int height, int* stream_id);
+/* Waits for the stream's queued frames, then frees its memory. */
+int bmfr_server_close_stream(bmfr_server* server, int stream_id);
+int bmfr_server_stream_inputs(bmfr_server* server, int stream_id, bmfr_frame_inputs* inputs);
+
+/* Queues the stream's next frame.  io: the frame's device buffers (they and
+ * the previous G-buffer pointers must stay valid until the request
+ * completes); NULL uses the stream's input slots, which the caller fills for
+ * one frame at a time (after the previous request completed).  io->result,
+ * if not NULL, receives the output.  matrix/offset: host memory, copied.
+ * Returns a request id. */
+int bmfr_server_submit(bmfr_server* server, int stream_id, const bmfr_frame_io* io, const float* matrix,
+                       const float* offset, uint64_t* request_id);
+/* done = 1 once the request's step has finished on the GPU; latency from
+ * submission to completion. */
+int bmfr_server_poll(bmfr_server* server, uint64_t request_id, int* done, double* latency_ms);
+/* Blocks until every submitted request has completed (or timeout_ms passes:
+ * BMFR_E_TIMEOUT). */
+int bmfr_server_drain(bmfr_server* server, double timeout_ms);
+int bmfr_server_stats_get(bmfr_server* server, bmfr_server_stats* stats);
+int bmfr_server_stats_reset(bmfr_server* server);
+/* The batch underneath (read-only use while the server runs). */
+bmfr_batch* bmfr_server_batch(bmfr_server* server);
+/* bmfr_batch_set_tuning, serialised with the server's steps. */
+int bmfr_server_set_tuning(bmfr_server* server, const bmfr_batch_tuning* tuning);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,79 @@
+"""The request server (continuous batching over the many-stream engine).
+
+Frames of several streams are submitted while earlier steps run; every
+result must equal what the stream's own plan produces alone (same
+parameters, fused pipeline), streams are admitted against the memory budget,
+and the statistics account for every request.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import bmfr_b200 as B
+from test_batch import SIZES, Stream
+
+pytestmark = pytest.mark.gpu
+
+
+def test_results_alone_and_in_the_mix(cuda):
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
+    server = B.Server(params)
+    ids = [server.open_stream(s.w, s.h) for s in streams]
+    frames = 5
+    for s in streams:   # render every frame up front; submissions must not wait on the host renderer
+        s.frame(frames - 1)
+    outs = {}
+
+    def client(k):
+        s = streams[k]
+        rng = np.random.default_rng(k)
+        for f in range(frames):
+            out = torch.empty(s.w * s.h * 3, dtype=torch.float32, device=cuda)
+            outs[(k, f)] = out
+            io = s.io(f)
+            io.result = out.data_ptr()
+            server.submit(ids[k], s.sc.prev_camera(f), s.sc.pixel_offset(f), io=io)
+            time.sleep(float(rng.uniform(0.0, 0.004)))   # arrivals interleave with steps
+
+    threads = [threading.Thread(target=client, args=(k,)) for k in range(len(streams))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    server.drain(60000)
+    torch.cuda.synchronize()
+    st = server.stats()
+    assert st["requests_completed"] == st["requests_submitted"] == frames * len(streams)
+    assert st["p99_latency_ms"] >= st["p50_latency_ms"] > 0
+    # Alone: each stream through its own plan.
+    for k, s in enumerate(streams):
+        for f in range(frames):
+            want = s.plan_step(f).cpu().numpy()
+            np.testing.assert_array_equal(outs[(k, f)].cpu().numpy(), want, err_msg=f"stream {k} frame {f}")
+    server.close()
+
+
+def test_admission_against_the_budget(cuda):
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    need = B.Batch.stream_bytes(params, 320, 180)
+    server = B.Server(params, memory_budget_bytes=2 * need + need // 2)
+    a = server.open_stream(320, 180)
+    b = server.open_stream(320, 180)
+    with pytest.raises(B.BmfrError) as e:
+        server.open_stream(320, 180)
+    assert e.value.status == B._native.BMFR_E_BUDGET
+    server.close_stream(a)                  # memory frees up ...
+    c = server.open_stream(320, 180)        # ... and the next stream is admitted (in the freed slot)
+    assert c != b
+    st = server.stats()
+    assert st["streams_admitted"] == 3 and st["streams_rejected"] == 1
+    server.close_stream(c)
+    with pytest.raises(B.BmfrError):
+        server.submit(c, np.eye(4), [0.5, 0.5])   # closed stream
+    with pytest.raises(B.BmfrError):
+        server.submit(999, np.eye(4), [0.5, 0.5])   # never opened
+    server.close()
