@@ -16,12 +16,12 @@ import numpy as np
 
 from . import _native
 from ._native import (BatchTuning, ServerConfig, ServerStats, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check,
-                      lib, PIPELINE_FUSED, PIPELINE_STAGED)
+                      lib, PIPELINE_FUSED, PIPELINE_STAGED, QR_CHOLESKY2, QR_HOUSEHOLDER, QR_REFERENCE)
 
 __all__ = [
     "Plan", "Batch", "Server", "Scene", "BmfrError", "default_params", "block_offsets",
     "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
-    "PIPELINE_FUSED", "PIPELINE_STAGED", "library_path",
+    "PIPELINE_FUSED", "PIPELINE_STAGED", "QR_REFERENCE", "QR_CHOLESKY2", "QR_HOUSEHOLDER", "library_path",
 ]
 
 library_path = _native.library_path
@@ -348,6 +348,10 @@ class Batch:
             check(v, "bmfr_batch_stream_frame")
         return v
 
+    def reserve(self, nbytes: int) -> None:
+        """Grows the stream memory pool to at least nbytes (blocking)."""
+        check(lib.bmfr_batch_reserve(self.handle, int(nbytes)), "bmfr_batch_reserve")
+
     @property
     def bytes_in_use(self) -> int:
         return lib.bmfr_batch_bytes_in_use(self.handle)
@@ -413,9 +417,10 @@ class Server:
     (include/bmfr_batch.h, bmfr_server_*)."""
 
     def __init__(self, params: Params | None = None, memory_budget_bytes: int = 0, max_streams_per_step: int = 0,
-                 own_inputs: bool = False, **overrides):
+                 own_inputs: bool = False, max_steps_in_flight: int = 0, reserve_bytes: int = 0, **overrides):
         self.params = params if params is not None else default_params(pipeline=PIPELINE_FUSED, **overrides)
-        cfg = ServerConfig(int(memory_budget_bytes), int(max_streams_per_step), int(own_inputs))
+        cfg = ServerConfig(int(memory_budget_bytes), int(max_streams_per_step), int(own_inputs),
+                           int(max_steps_in_flight), int(reserve_bytes))
         h = C.c_void_p()
         check(lib.bmfr_server_create(C.byref(self.params), C.byref(cfg), C.byref(h)), "bmfr_server_create")
         self._h = h

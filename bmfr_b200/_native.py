@@ -26,6 +26,10 @@ BMFR_E_TOO_LARGE = -10
 PIPELINE_STAGED = 0
 PIPELINE_FUSED = 1
 
+QR_REFERENCE = 0      # the reference's Householder sequence and binary16 rounding
+QR_CHOLESKY2 = 1      # precision form: CholeskyQR2 in FP32
+QR_HOUSEHOLDER = 2    # precision form: the Householder sequence in FP32
+
 
 class Params(C.Structure):
     _fields_ = [
@@ -80,7 +84,8 @@ class BatchTuning(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_streams_per_step", C.c_int), ("own_inputs", C.c_int)]
+    _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_streams_per_step", C.c_int), ("own_inputs", C.c_int),
+                ("max_steps_in_flight", C.c_int), ("reserve_bytes", C.c_size_t)]
 
 
 class ServerStats(C.Structure):
@@ -147,6 +152,7 @@ def _load() -> C.CDLL:
         "bmfr_batch_reset_stream": (i, [vp, i]),
         "bmfr_batch_stream_frame": (i, [vp, i]),
         "bmfr_batch_bytes_in_use": (C.c_size_t, [vp]),
+        "bmfr_batch_reserve": (i, [vp, C.c_size_t]),
         "bmfr_batch_stream_inputs": (i, [vp, i, C.POINTER(FrameInputs)]),
         "bmfr_batch_step": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, vp]),
         "bmfr_batch_stream_result": (i, [vp, i, C.POINTER(vp)]),

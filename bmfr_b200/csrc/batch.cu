@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(256) k_batch_noise(const BatchStepDesc* __rest
 // depth 0: blocks are taken from a global atomic queue; depth > 0: block
 // blockIdx.x + k * gridDim.x, with the inputs of the CTA's next `depth`
 // blocks prefetched into L2 while it fits the current one.
-template <bool ROUND, bool HALF_TMP, typename HistT>
-__global__ void __launch_bounds__(256, ROUND ? 3 : 2)
+template <int METHOD, bool HALF_TMP, typename HistT>
+__global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2)
     k_batch_blocks(const BatchStepDesc* __restrict__ d, int* __restrict__ counter, int depth) {
     __shared__ FitterSmem sm;
     __shared__ float w_s[kFeatures * 3], mm_s[kScaled * 2];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256, ROUND ? 3 : 2)
             const int ahead = item + depth * (int)gridDim.x;
             if (threadIdx.x < 32 && ahead < nb) prefetch_block_inputs(d, ahead);
             const int s = stream_of_block(d, item);
-            fused_block_body<ROUND, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
+            fused_block_body<METHOD, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
             __syncthreads();
         }
     } else {
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256, ROUND ? 3 : 2)
             const int item = item_s;
             if (item >= nb) break;
             const int s = stream_of_block(d, item);
-            fused_block_body<ROUND, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
+            fused_block_body<METHOD, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
             __syncthreads();
         }
     }
@@ -132,42 +132,52 @@ cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaS
     return cudaGetLastError();
 }
 
-template <bool ROUND, bool HALF_TMP, typename HistT>
+template <int METHOD, bool HALF_TMP, typename HistT>
 static cudaError_t launch_blocks_t(const BatchStepDesc* desc, int* counter, int depth, int grid, cudaStream_t s) {
-    k_batch_blocks<ROUND, HALF_TMP, HistT><<<grid, kLocal, 0, s>>>(desc, counter, depth);
+    k_batch_blocks<METHOD, HALF_TMP, HistT><<<grid, kLocal, 0, s>>>(desc, counter, depth);
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, bool fp32_qr, bool half_tmp,
-                                bool half_history, int depth, int grid, cudaStream_t s) {
-    if (half_history) {
-        if (half_tmp && !fp32_qr) return launch_blocks_t<true, true, __half>(desc, counter, depth, grid, s);
-        if (half_tmp) return launch_blocks_t<false, true, __half>(desc, counter, depth, grid, s);
-        return launch_blocks_t<false, false, __half>(desc, counter, depth, grid, s);
-    }
-    if (half_tmp && !fp32_qr) return launch_blocks_t<true, true, float>(desc, counter, depth, grid, s);
-    if (half_tmp) return launch_blocks_t<false, true, float>(desc, counter, depth, grid, s);
-    return launch_blocks_t<false, false, float>(desc, counter, depth, grid, s);
+template <int METHOD, bool HALF_TMP, typename HistT>
+static int occupancy_t() {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<METHOD, HALF_TMP, HistT>, kLocal, 0);
+    return per_sm;
 }
 
-int batch_block_occupancy(bool fp32_qr, bool half_tmp, bool half_history) {
-    int per_sm = 0;
-    if (half_history) {
-        if (half_tmp && !fp32_qr)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<true, true, __half>, kLocal, 0);
-        else if (half_tmp)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<false, true, __half>, kLocal, 0);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<false, false, __half>, kLocal, 0);
-    } else {
-        if (half_tmp && !fp32_qr)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<true, true, float>, kLocal, 0);
-        else if (half_tmp)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<false, true, float>, kLocal, 0);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<false, false, float>, kLocal, 0);
-    }
-    return per_sm;
+// The kernel instance for (qr, half_tmp, HistT) handed to F::run.
+template <typename HistT, typename F>
+static auto dispatch_blocks(int qr, bool half_tmp, F&& f) {
+    if (!half_tmp) return f.template run<kFitReference, false, HistT>();
+    if (qr == kFitCholQR2) return f.template run<kFitCholQR2, true, HistT>();
+    if (qr == kFitHouseholder32) return f.template run<kFitHouseholder32, true, HistT>();
+    return f.template run<kFitReference, true, HistT>();
+}
+
+struct LaunchBlocks {
+    const BatchStepDesc* desc;
+    int* counter;
+    int depth, grid;
+    cudaStream_t s;
+    template <int M, bool H, typename T>
+    cudaError_t run() const { return launch_blocks_t<M, H, T>(desc, counter, depth, grid, s); }
+};
+
+struct Occupancy {
+    template <int M, bool H, typename T>
+    int run() const { return occupancy_t<M, H, T>(); }
+};
+
+cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, int qr, bool half_tmp,
+                                bool half_history, int depth, int grid, cudaStream_t s) {
+    const LaunchBlocks l{desc, counter, depth, grid, s};
+    if (half_history) return dispatch_blocks<__half>(qr, half_tmp, l);
+    return dispatch_blocks<float>(qr, half_tmp, l);
+}
+
+int batch_block_occupancy(int qr, bool half_tmp, bool half_history) {
+    if (half_history) return dispatch_blocks<__half>(qr, half_tmp, Occupancy{});
+    return dispatch_blocks<float>(qr, half_tmp, Occupancy{});
 }
 
 template <int TW, int TH>

@@ -37,10 +37,11 @@ struct BatchTuning {
 // captured graph serves every step whatever streams take part.
 cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaStream_t s);
 // grid: persistent CTAs (from batch_block_occupancy and the tuning).
-cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, bool fp32_qr, bool half_tmp,
+// qr: bmfr_params.fp32_qr (FitMethod).
+cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, int qr, bool half_tmp,
                                 bool half_history, int depth, int grid, cudaStream_t s);
 cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const BatchTuning& t, int sms,
                              cudaStream_t s);
-int batch_block_occupancy(bool fp32_qr, bool half_tmp, bool half_history);
+int batch_block_occupancy(int qr, bool half_tmp, bool half_history);
 
 }  // namespace bmfr

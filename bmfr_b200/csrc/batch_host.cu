@@ -19,13 +19,14 @@ using bmfr::fail;
 namespace {
 
 struct StreamSlot {
-    bool used = false;
+    bool used = false;    // taken (possibly still being allocated)
+    bool ready = false;   // allocated: steps may name it
     int width = 0, height = 0;
     bmfr::Geometry g{};
     int frame = 0;
     bool own_inputs = false;
     size_t bytes = 0;
-    std::vector<void*> allocs;
+    void* base = nullptr;   // one pool allocation holds every buffer below
     // histories (HistT per the batch's half_history) and per-frame buffers
     void* noisy_acc[2] = {nullptr, nullptr};
     void* acc_filt[2] = {nullptr, nullptr};
@@ -45,19 +46,52 @@ struct StreamSlot {
     float* noisy = nullptr;
 };
 
-size_t stream_bytes(const bmfr_params& p, int w, int h, bool own_inputs) {
+// Lays the stream's buffers out from `base` (256-byte aligned pieces) and
+// returns the total size; with base == nullptr only the size is computed.
+size_t carve(StreamSlot& s, const bmfr_params& p, int w, int h, bool own_inputs, char* base) {
     const bmfr::Geometry g = bmfr::make_geometry(w, h);
     const size_t px = (size_t)w * h;
     const size_t hist = px * 3 * (p.half_history ? 2 : 4);
-    size_t b = 6 * hist + 2 * px + px * 8 + px + px * 12 + px * 12;
-    b += (size_t)g.blocks * (bmfr::kFeatures * 3 + bmfr::kScaled * 2) * 4 + bmfr::kNoiseTableBytes;
-    if (own_inputs) b += px * 12 * 6;
-    return b;
+    size_t off = 0;
+    auto take = [&](size_t n, auto** ptr) {
+        *ptr = base ? reinterpret_cast<std::remove_pointer_t<decltype(ptr)>>(base + off) : nullptr;
+        off += (n + 255) & ~size_t(255);
+    };
+    for (int i = 0; i < 2; ++i) {
+        take(hist, &s.noisy_acc[i]);
+        take(hist, &s.acc_filt[i]);
+        take(hist, &s.result[i]);
+        take(px, &s.spp[i]);
+    }
+    take(px * 8, &s.prev_pix);
+    take(px, &s.accept);
+    take(px * 12, &s.tone_mapped);
+    take(px * 12, &s.result_f32);
+    take((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &s.weights);
+    take((size_t)g.blocks * bmfr::kScaled * 2 * 4, &s.mins_maxs);
+    take(bmfr::kNoiseTableBytes, &s.noise);
+    if (own_inputs) {
+        for (int i = 0; i < 2; ++i) {
+            take(px * 12, &s.normals[i]);
+            take(px * 12, &s.positions[i]);
+        }
+        take(px * 12, &s.albedo);
+        take(px * 12, &s.noisy);
+    }
+    return off;
+}
+
+size_t stream_bytes(const bmfr_params& p, int w, int h, bool own_inputs) {
+    StreamSlot tmp;
+    return carve(tmp, p, w, h, own_inputs, nullptr);
 }
 
 }  // namespace
 
 struct bmfr_batch {
+    // Guards the slot table, `used` and `last`: streams may be added and
+    // removed from other threads while a step is being formed.
+    mutable std::mutex mu;
     bmfr_params p{};
     int device = 0;
     int sms = 0;
@@ -71,6 +105,12 @@ struct bmfr_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaEvent_t done[2] = {nullptr, nullptr};
     bool graphs_valid = false;
+    // Stream memory comes from a device pool in stream order on mem_stream,
+    // so that streams join and leave without a device-wide synchronisation;
+    // steps wait for mem_ready (the last allocation and its zeroing).
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t mem_stream = nullptr;
+    cudaEvent_t mem_ready = nullptr;
     int next = 0;
     int last = -1;
 };
@@ -86,13 +126,18 @@ int check_batch(const bmfr_batch* b) {
 }
 
 int check_slot(const bmfr_batch* b, int slot) {
-    if (slot < 0 || slot >= BMFR_BATCH_MAX_STREAMS || !b->slots[slot].used)
+    if (slot < 0 || slot >= BMFR_BATCH_MAX_STREAMS || !b->slots[slot].used || !b->slots[slot].ready)
         return fail(BMFR_E_NOT_FOUND, "no stream in slot " + std::to_string(slot));
     return BMFR_OK;
 }
 
+// Returns the slot's memory to the pool once every step launched so far is
+// done with it (steps run in order, so the last one is enough).
 void free_slot(bmfr_batch* b, StreamSlot& s) {
-    for (void* p : s.allocs) cudaFree(p);
+    if (s.base) {
+        if (b->last >= 0) cudaStreamWaitEvent(b->mem_stream, b->done[b->last], 0);
+        cudaFreeAsync(s.base, b->mem_stream);
+    }
     b->used -= s.bytes;
     s = StreamSlot();
 }
@@ -126,7 +171,7 @@ int build_graphs(bmfr_batch* b) {
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(int), cs);
         if (e == cudaSuccess) e = bmfr::launch_batch_noise(b->d_desc, BMFR_BATCH_MAX_STREAMS, cs);
         if (e == cudaSuccess)
-            e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr != 0, half_tmp,
+            e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr, half_tmp,
                                           b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms, cs);
         if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
@@ -229,6 +274,7 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
     if (!params || !out) return fail(BMFR_E_INVALID, "NULL argument");
     *out = nullptr;
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    if (params->fp32_qr < 0 || params->fp32_qr > 2) return fail(BMFR_E_INVALID, "fp32_qr must be 0, 1 or 2");
     int dev = -1;
     if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) {
         cudaGetLastError();
@@ -240,7 +286,7 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
     b->device = dev;
     b->budget = memory_budget_bytes;
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-    b->block_occupancy = std::max(1, bmfr::batch_block_occupancy(params->fp32_qr != 0,
+    b->block_occupancy = std::max(1, bmfr::batch_block_occupancy(params->fp32_qr,
                                                                  params->use_half_precision_in_tmp_data != 0,
                                                                  params->half_history != 0));
     cudaError_t e = cudaMalloc(&b->d_desc, sizeof(bmfr::BatchStepDesc));
@@ -250,6 +296,21 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
         if (e == cudaSuccess) std::memset(b->h_desc[k], 0, sizeof(bmfr::BatchStepDesc));
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done[k], cudaEventDisableTiming);
     }
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        e = cudaMemPoolCreate(&b->pool, &props);
+    }
+    if (e == cudaSuccess) {
+        // Freed stream memory stays with the pool for the next stream.
+        uint64_t keep = ~uint64_t(0);
+        e = cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->mem_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->mem_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(b->mem_ready, b->mem_stream);
     if (e != cudaSuccess) {
         bmfr_batch_destroy(b);
         return cuda_fail(e, "batch allocation");
@@ -269,6 +330,10 @@ int bmfr_batch_destroy(bmfr_batch* b) {
         if (b->h_desc[k]) cudaFreeHost(b->h_desc[k]);
         if (b->done[k]) cudaEventDestroy(b->done[k]);
     }
+    if (b->mem_stream) cudaStreamSynchronize(b->mem_stream);
+    if (b->mem_ready) cudaEventDestroy(b->mem_ready);
+    if (b->mem_stream) cudaStreamDestroy(b->mem_stream);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
     if (b->d_desc) cudaFree(b->d_desc);
     if (b->d_counters) cudaFree(b->d_counters);
     delete b;
@@ -283,77 +348,57 @@ int bmfr_batch_add_stream(bmfr_batch* b, int width, int height, int own_inputs, 
     const bmfr::Geometry g = bmfr::make_geometry(width, height);
     if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
         return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
-    int k = 0;
-    while (k < BMFR_BATCH_MAX_STREAMS && b->slots[k].used) ++k;
-    if (k == BMFR_BATCH_MAX_STREAMS) return fail(BMFR_E_TOO_LARGE, "all stream slots are in use");
     const size_t bytes = stream_bytes(b->p, width, height, own_inputs != 0);
-    if (b->budget && b->used + bytes > b->budget)
-        return fail(BMFR_E_BUDGET, "stream needs " + std::to_string(bytes) + " bytes, " +
-                                       std::to_string(b->budget - b->used) + " left in the budget");
+    int k = 0;
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        while (k < BMFR_BATCH_MAX_STREAMS && b->slots[k].used) ++k;
+        if (k == BMFR_BATCH_MAX_STREAMS) return fail(BMFR_E_TOO_LARGE, "all stream slots are in use");
+        if (b->budget && b->used + bytes > b->budget)
+            return fail(BMFR_E_BUDGET, "stream needs " + std::to_string(bytes) + " bytes, " +
+                                           std::to_string(b->budget - b->used) + " left in the budget");
+        b->slots[k].used = true;   // reserved; steps cannot name it until ready
+        b->slots[k].bytes = bytes;
+        b->used += bytes;
+    }
+    // The allocation may have to grow the pool, which can take a while:
+    // steps of the other streams go on meanwhile.
+    void* base = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&base, bytes, b->pool, b->mem_stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, bytes, b->mem_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b->mem_ready, b->mem_stream);
+    std::lock_guard<std::mutex> lk(b->mu);
     StreamSlot& s = b->slots[k];
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (base) cudaFreeAsync(base, b->mem_stream);
+        b->used -= bytes;
+        s = StreamSlot();
+        return fail(BMFR_E_NOMEM, "device allocation for the stream failed: " + std::string(cudaGetErrorString(e)));
+    }
     s.width = width;
     s.height = height;
     s.g = g;
     s.frame = 0;
     s.own_inputs = own_inputs != 0;
-    const size_t px = (size_t)width * height;
-    const size_t hist = px * 3 * (b->p.half_history ? 2 : 4);
-    bool ok = true;
-    auto alloc = [&](size_t n, auto** ptr) {
-        if (!ok) return;
-        void* p = nullptr;
-        if (cudaMalloc(&p, n) != cudaSuccess) {
-            cudaGetLastError();
-            ok = false;
-            return;
-        }
-        cudaMemset(p, 0, n);
-        s.allocs.push_back(p);
-        *ptr = static_cast<std::remove_pointer_t<decltype(ptr)>>(p);
-    };
-    for (int i = 0; i < 2; ++i) {
-        alloc(hist, &s.noisy_acc[i]);
-        alloc(hist, &s.acc_filt[i]);
-        alloc(hist, &s.result[i]);
-        alloc(px, &s.spp[i]);
-    }
-    alloc(px * 8, &s.prev_pix);
-    alloc(px, &s.accept);
-    alloc(px * 12, &s.tone_mapped);
-    alloc(px * 12, &s.result_f32);
-    alloc((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &s.weights);
-    alloc((size_t)g.blocks * bmfr::kScaled * 2 * 4, &s.mins_maxs);
-    alloc(bmfr::kNoiseTableBytes, &s.noise);
-    if (s.own_inputs) {
-        for (int i = 0; i < 2; ++i) {
-            alloc(px * 12, &s.normals[i]);
-            alloc(px * 12, &s.positions[i]);
-        }
-        alloc(px * 12, &s.albedo);
-        alloc(px * 12, &s.noisy);
-    }
-    s.bytes = bytes;
-    s.used = true;
-    b->used += bytes;
-    if (!ok) {
-        free_slot(b, s);
-        return fail(BMFR_E_NOMEM, "device allocation for the stream failed");
-    }
+    s.base = base;
+    carve(s, b->p, width, height, s.own_inputs, static_cast<char*>(base));
+    s.ready = true;
     *slot = k;
     return BMFR_OK;
 }
 
 int bmfr_batch_remove_stream(bmfr_batch* b, int slot) {
     if (int st = check_batch(b)) return st;
+    std::lock_guard<std::mutex> lk(b->mu);
     if (int st = check_slot(b, slot)) return st;
-    for (cudaEvent_t e : b->done)   // no step may still use its buffers
-        if (e) cudaEventSynchronize(e);
-    free_slot(b, b->slots[slot]);
+    free_slot(b, b->slots[slot]);   // in stream order after the steps that use it
     return BMFR_OK;
 }
 
 int bmfr_batch_reset_stream(bmfr_batch* b, int slot) {
     if (!b) return fail(BMFR_E_INVALID, "batch is NULL");
+    std::lock_guard<std::mutex> lk(b->mu);
     if (int st = check_slot(b, slot)) return st;
     b->slots[slot].frame = 0;
     return BMFR_OK;
@@ -361,17 +406,39 @@ int bmfr_batch_reset_stream(bmfr_batch* b, int slot) {
 
 int bmfr_batch_stream_frame(const bmfr_batch* b, int slot) {
     if (!b) return fail(BMFR_E_INVALID, "batch is NULL");
+    std::lock_guard<std::mutex> lk(b->mu);
     if (int st = check_slot(b, slot)) return st;
     return b->slots[slot].frame;
 }
 
-size_t bmfr_batch_bytes_in_use(const bmfr_batch* b) { return b ? b->used : 0; }
+int bmfr_batch_reserve(bmfr_batch* b, size_t bytes) {
+    if (int st = check_batch(b)) return st;
+    if (bytes == 0) return BMFR_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, b->pool, b->mem_stream);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, b->mem_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->mem_stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BMFR_E_NOMEM, "reserving stream memory failed: " + std::string(cudaGetErrorString(e)));
+    }
+    return BMFR_OK;
+}
+
+size_t bmfr_batch_bytes_in_use(const bmfr_batch* b) {
+    if (!b) return 0;
+    std::lock_guard<std::mutex> lk(b->mu);
+    return b->used;
+}
 
 int bmfr_batch_stream_inputs(bmfr_batch* b, int slot, bmfr_frame_inputs* in) {
     if (!b || !in) return fail(BMFR_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(b->mu);
     if (int st = check_slot(b, slot)) return st;
     StreamSlot& s = b->slots[slot];
     if (!s.own_inputs) return fail(BMFR_E_STATE, "stream was added without input slots");
+    // The caller writes these on its own streams: the allocation must exist.
+    if (cudaError_t e = cudaEventSynchronize(b->mem_ready); e != cudaSuccess) return cuda_fail(e, "stream memory");
     const int cur = s.frame & 1;
     in->albedo = s.albedo;
     in->normals = s.normals[cur];
@@ -385,22 +452,25 @@ int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io*
     if (int st = check_batch(b)) return st;
     if (n <= 0 || n > BMFR_BATCH_MAX_STREAMS || !slots || !matrices || !offsets)
         return fail(BMFR_E_INVALID, "step: bad stream list");
-    for (int i = 0; i < n; ++i) {
-        if (int st = check_slot(b, slots[i])) return st;
-        for (int j = 0; j < i; ++j)
-            if (slots[j] == slots[i]) return fail(BMFR_E_INVALID, "step: a stream is listed twice");
-    }
     if (!b->graphs_valid)
         if (int st = build_graphs(b)) return st;
     const int k = b->next;
     cudaError_t e = cudaEventSynchronize(b->done[k]);   // description buffer k is free again
     if (e != cudaSuccess) return cuda_fail(e, "step: waiting for an earlier step");
+    std::lock_guard<std::mutex> lk(b->mu);
+    for (int i = 0; i < n; ++i) {
+        if (int st = check_slot(b, slots[i])) return st;
+        for (int j = 0; j < i; ++j)
+            if (slots[j] == slots[i]) return fail(BMFR_E_INVALID, "step: a stream is listed twice");
+    }
     if (int st = fill_desc(b, b->h_desc[k], n, slots, io, matrices, offsets)) return st;
     cudaStream_t s = (cudaStream_t)stream;
     if (b->last >= 0) {
         e = cudaStreamWaitEvent(s, b->done[b->last], 0);
         if (e != cudaSuccess) return cuda_fail(e, "step: ordering after the previous step");
     }
+    e = cudaStreamWaitEvent(s, b->mem_ready, 0);   // streams added since are allocated and zeroed
+    if (e != cudaSuccess) return cuda_fail(e, "step: ordering after stream allocation");
     e = cudaGraphLaunch(b->graph[k], s);
     if (e == cudaSuccess) e = cudaEventRecord(b->done[k], s);
     if (e != cudaSuccess) return cuda_fail(e, "step: graph launch");
@@ -412,6 +482,7 @@ int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io*
 
 int bmfr_batch_stream_result(const bmfr_batch* b, int slot, const float** result) {
     if (!b || !result) return fail(BMFR_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(b->mu);
     if (int st = check_slot(b, slot)) return st;
     *result = b->slots[slot].result_f32;
     return BMFR_OK;

@@ -167,6 +167,7 @@ int validate(const bmfr_params* params, int width, int height) {
     if (g.MW - 3 > 2 * width - 1 || g.MH - 3 > 2 * height - 1)
         return fail(BMFR_E_UNSUPPORTED, "image too small for the mirrored 16-pixel margin");
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
+    if (params->fp32_qr < 0 || params->fp32_qr > 2) return fail(BMFR_E_INVALID, "fp32_qr must be 0, 1 or 2");
     return BMFR_OK;
 }
 
@@ -185,6 +186,7 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
     if (params->pipeline != BMFR_PIPELINE_STAGED && params->pipeline != BMFR_PIPELINE_FUSED)
         return fail(BMFR_E_INVALID, "unknown pipeline");
+    if (params->fp32_qr < 0 || params->fp32_qr > 2) return fail(BMFR_E_INVALID, "fp32_qr must be 0, 1 or 2");
     if (!(params->blend_alpha > 0.f) || !(params->second_blend_alpha > 0.f))
         return fail(BMFR_E_INVALID, "blend factors must be positive");
     int device = -1;
@@ -299,7 +301,7 @@ int bmfr_fitter(const bmfr_plan* plan, float* weights, float* mins_maxs, const v
     if (frame_number < 0) return fail(BMFR_E_INVALID, "fitter: negative frame number");
     cudaError_t e = bmfr::launch_fitter(plan->g, frame_number, bmfr::make_noise_const(plan->p.noise_amount),
                                         tmp_data, plan->p.use_half_precision_in_tmp_data != 0,
-                                        plan->p.fp32_qr != 0, weights, mins_maxs, nullptr, plan->dev_status,
+                                        plan->p.fp32_qr, weights, mins_maxs, nullptr, plan->dev_status,
                                         (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter launch");
 }
@@ -326,7 +328,7 @@ int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height, float*
     const bmfr::Geometry g = bmfr::make_geometry(width, height);
     cudaError_t e = bmfr::launch_fitter_static(g, frame_number, bmfr::make_noise_const(params->noise_amount),
                                                tmp_data, params->use_half_precision_in_tmp_data != 0,
-                                               params->fp32_qr != 0, weights, mins_maxs, (cudaStream_t)stream);
+                                               params->fp32_qr, weights, mins_maxs, (cudaStream_t)stream);
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter_noalloc launch");
 }
 
@@ -444,7 +446,7 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         fb.noise = plan->noise_table;
         if (e == cudaSuccess)
             e = bmfr::launch_fused_block(g, a, bmfr::make_noise_const(plan->p.noise_amount),
-                                         plan->p.second_blend_alpha, plan->p.fp32_qr != 0, half_hist, fb, s);
+                                         plan->p.second_blend_alpha, plan->p.fp32_qr, half_hist, fb, s);
         mark(2);
     } else {
         if (e == cudaSuccess)
@@ -454,7 +456,7 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         mark(1);
         if (e == cudaSuccess)
             e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
-                                    plan->p.fp32_qr != 0, plan->weights, plan->mins_maxs, plan->noise_table,
+                                    plan->p.fp32_qr, plan->weights, plan->mins_maxs, plan->noise_table,
                                     plan->dev_status, s);
         mark(2);
         if (!half_hist) {

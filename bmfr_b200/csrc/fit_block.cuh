@@ -50,6 +50,16 @@ struct FitterSmem {
     float rhs[10][3];      // rows 0..9 of the three colour columns
     float part2[13 * 8];   // second-stage sums, 8 per batched value
     float rowc[13];        // the precision form: row `col` of every column
+    float inv1[10];        // CholeskyQR2: reciprocals of R1's and R2's diagonals,
+    float inv2[10];        //   and the diagonal of the Gram matrix being factored
+    float diag[10];
+};
+
+// How the block's least-squares system is solved.
+enum FitMethod : int {
+    kFitReference = 0,     // the reference's Householder sequence and rounding
+    kFitCholQR2 = 1,       // precision form: CholeskyQR2 in FP32
+    kFitHouseholder32 = 2  // precision form: the Householder sequence in FP32
 };
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -491,8 +501,240 @@ __device__ __forceinline__ void fit_columns_fast(Tile<false>& t, int id, const f
     }
 }
 
-// FAST (float tile only): the precision form's FP32 QR (fit_columns_fast).
-template <bool HALF, bool FAST = false>
+// ---------------------------------------------------------------------------
+// The precision form's default fit: CholeskyQR2 in FP32.
+//
+// The ten feature columns A (1024 x 10, scaled, with the noise of features
+// 1..9) are factored A = Q R by two Gram passes (CholeskyQR2, Fukaya,
+// Nakatsukasa, Yanagisawa and Yamamoto, 2014): R1 = chol(A^T A),
+// Q1 = A R1^-1 row by row in registers, R2 = chol(Q1^T Q1), R = R2 R1.  The
+// colour columns B ride along in the second pass: Q1^T B is reduced with
+// Q1^T Q1, and the Cholesky of that augmented Gram matrix returns
+// z = R2^-T Q1^T B = Q^T B, the rows 0..9 of the colour columns that the
+// reference's Householder sequence leaves.  The weights are R^-1 z, by two
+// triangular solves (R2, then R1).
+//
+// Each pass is one batched reduction of its Gram entries over the CTA, where
+// the Householder sequence reduces once per column; the two Cholesky
+// factorisations and the solves run in warp 0 with lane j holding column j.
+// The noise of features 1..9 keeps cond(A) below about 1e3, so the first
+// pass's FP32 Gram matrix stays positive definite, and the second pass,
+// whose matrix is within rounding of the identity, restores the accuracy the
+// first one loses: the fitted colours match the fp64 fitter more closely
+// than the FP32 Householder sequence does on blocks with fireflies, whose
+// large colour norms scale every rounding error of the sequence.  A pivot
+// below 2^-20 of its column's squared norm marks the column dependent: its
+// row of R and its weight are zero.
+
+constexpr int kGram1 = kFeatures * (kFeatures + 1) / 2;   // 55 entries of A^T A
+constexpr int kGram2 = kGram1 + kFeatures * 3;             // + Q1^T B: 85
+constexpr int kGramStride = 96;                            // per warp in sm.part
+constexpr int kGramChunk = 16;                             // entries reduced per butterfly
+
+// One step of the transposing butterfly over lanes l and l ^ X: each lane
+// sends half of its 2H values and keeps the other half summed over the pair.
+template <int H, int X, int N>
+__device__ __forceinline__ void transpose_step(float (&v)[N], int lane) {
+    const bool up = lane & X;
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+        const float send = up ? v[k] : v[k + H], keep = up ? v[k + H] : v[k];
+        v[k] = keep + __shfl_xor_sync(kFull, send, X);
+    }
+}
+
+// Sum over the warp of C = 16 or 32 values per lane (C - 1 shuffles).  On
+// return v[0] holds entry lane (C = 32) or lane >> 1 (C = 16, both lanes of
+// a pair hold it).
+template <int C>
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[C]) {
+    const int lane = threadIdx.x & 31;
+    if constexpr (C == 32) {
+        transpose_step<16, 16>(v, lane);
+        transpose_step<8, 8>(v, lane);
+        transpose_step<4, 4>(v, lane);
+        transpose_step<2, 2>(v, lane);
+        transpose_step<1, 1>(v, lane);
+    } else {
+        transpose_step<8, 16>(v, lane);
+        transpose_step<4, 8>(v, lane);
+        transpose_step<2, 4>(v, lane);
+        transpose_step<1, 2>(v, lane);
+        v[0] = v[0] + __shfl_xor_sync(kFull, v[0], 1);
+    }
+    return v[0];
+}
+
+// Sum of a_i * a_j over the thread's four rows.
+__device__ __forceinline__ float gram4(const Tile<false>& t, int i, int j) {
+    const float2 g = fma2(t.p[i][1], t.p[j][1], mul2(t.p[i][0], t.p[j][0]));
+    return g.x + g.y;
+}
+
+// Gram entries [BASE, BASE + C): entry tri(i, j) = j(j+1)/2 + i (i <= j) of
+// the features' Gram matrix, then (second pass) 55 + 10c + i = column i
+// against colour c.  Each warp's sums land in sm.part[warp * 96 + entry].
+template <int BASE, int C, bool PASS2>
+__device__ __forceinline__ void gram_chunk(const Tile<false>& t, FitterSmem& sm) {
+    float v[C];
+#pragma unroll
+    for (int k = 0; k < C; ++k) v[k] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kFeatures; ++j) {
+#pragma unroll
+        for (int i = 0; i < kFeatures; ++i) {
+            const int e = j * (j + 1) / 2 + i;
+            if (i <= j && e >= BASE && e < BASE + C) v[e - BASE] = gram4(t, i, j);
+        }
+    }
+    if (PASS2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int i = 0; i < kFeatures; ++i) {
+                const int e = kGram1 + kFeatures * c + i;
+                if (e >= BASE && e < BASE + C) v[e - BASE] = gram4(t, i, kFeatures + c);
+            }
+        }
+    }
+    const float s = warp_transpose_sum<C>(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int e = BASE + (C == 32 ? lane : lane >> 1);
+    if ((C == 32 || (lane & 1) == 0) && e < (PASS2 ? kGram2 : kGram1)) sm.part[warp * kGramStride + e] = s;
+}
+
+// All Gram entries of a pass in chunks of C.
+template <int C, bool PASS2, int BASE = 0>
+__device__ __forceinline__ void gram_all(const Tile<false>& t, FitterSmem& sm) {
+    gram_chunk<BASE, C, PASS2>(t, sm);
+    if constexpr (BASE + C < (PASS2 ? kGram2 : kGram1)) gram_all<C, PASS2, BASE + C>(t, sm);
+}
+
+// Warp 0, after the barrier that follows gram_chunk: lane j < 10 gathers
+// column j of the Gram matrix (g[i], i <= j; zeros below) and stores its
+// diagonal entry in diag[j]; lanes 10..12 gather the colour column
+// c = lane - 10 of the second pass; other lanes zeros.
+template <bool PASS2>
+__device__ __forceinline__ void gram_columns(FitterSmem& sm, int lane, float (&g)[kFeatures]) {
+#pragma unroll
+    for (int i = 0; i < kFeatures; ++i) {
+        int e = -1;
+        if (lane < kFeatures) e = i <= lane ? lane * (lane + 1) / 2 + i : -1;
+        else if (PASS2 && lane < kFeatures + 3) e = kGram1 + kFeatures * (lane - kFeatures) + i;
+        float s = 0.0f;
+        if (e >= 0) {
+            const float* p = sm.part + e;
+            s = ((p[0] + p[kGramStride]) + (p[2 * kGramStride] + p[3 * kGramStride])) +
+                ((p[4 * kGramStride] + p[5 * kGramStride]) + (p[6 * kGramStride] + p[7 * kGramStride]));
+        }
+        g[i] = s;
+        if (i == lane) sm.diag[i] = s;
+    }
+    __syncwarp();
+}
+
+// Cholesky factorisation by one warp.  In: lane j < 10 holds column j of a
+// symmetric matrix (g[i], i <= j), lanes 10..12 right-hand columns, diag[k]
+// its diagonal.  Out: lane j holds column j of R (g[i] = R(i, j)), lanes
+// 10..12 hold R^-T times their column, and inv[k] = 1 / R(k, k) (0 for a
+// dependent column) in shared memory.
+__device__ __forceinline__ void chol_lanes(float (&g)[kFeatures], int lane, const float* diag, float* inv) {
+#pragma unroll
+    for (int k = 0; k < kFeatures; ++k) {
+        const float d = __shfl_sync(kFull, g[k], k);
+        const bool ok = d > 0x1p-20f * diag[k];
+        const float y = ok ? rsqrtf(d) : 0.0f;   // 1 / R(k, k)
+        const float r = d * y;
+        if (lane == 0) inv[k] = y;
+        if (lane == k) g[k] = r;
+        else if (lane > k) g[k] = g[k] * y;
+#pragma unroll
+        for (int i = 0; i < kFeatures; ++i) {
+            if (i > k) {
+                const float rki = __shfl_sync(kFull, g[k], i);
+                if (lane >= i) g[i] = __fmaf_rn(-rki, g[k], g[i]);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// The fit of a scaled block (float tile, min/max already applied).
+__device__ __forceinline__ void fit_columns_cqr2(Tile<false>& t, const float* __restrict__ noise, NoiseConst nc,
+                                                 FitterSmem& sm, float* __restrict__ weights_out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float2 hi = dup2(nc.hi);
+#pragma unroll
+    for (int k = 1; k < kFeatures; ++k) {   // noise of features 1..9 (bmfr.cl:625-627)
+        const float* r = noise + (k - 1) * 4 * kLocal + threadIdx.x;
+        t.p[k][0] = fma2(hi, make_float2(r[0], r[kLocal]), t.p[k][0]);
+        t.p[k][1] = fma2(hi, make_float2(r[2 * kLocal], r[3 * kLocal]), t.p[k][1]);
+    }
+    // Pass 1: R1 = chol(A^T A).
+    gram_all<kGramChunk, false>(t, sm);
+    __syncthreads();
+    if (warp == 0) {
+        float g[kFeatures];
+        gram_columns<false>(sm, lane, g);
+        chol_lanes(g, lane, sm.diag, sm.inv1);
+        if (lane < kFeatures) {
+#pragma unroll
+            for (int i = 0; i < kFeatures; ++i)
+                if (i <= lane) sm.Rm[lane][i] = g[i];
+        }
+    }
+    __syncthreads();
+    // Q1 = A R1^-1, one row at a time (forward substitution on row vectors).
+#pragma unroll
+    for (int j = 0; j < kFeatures; ++j) {
+        float2 a0 = t.p[j][0], a1 = t.p[j][1];
+#pragma unroll
+        for (int i = 0; i < j; ++i) {
+            const float2 r = dup2(-sm.Rm[j][i]);
+            a0 = fma2(r, t.p[i][0], a0);
+            a1 = fma2(r, t.p[i][1], a1);
+        }
+        const float2 y = dup2(sm.inv1[j]);
+        t.p[j][0] = mul2(a0, y);
+        t.p[j][1] = mul2(a1, y);
+    }
+    // Pass 2: R2 = chol(Q1^T Q1) and z = R2^-T Q1^T B.
+    gram_all<kGramChunk, true>(t, sm);
+    __syncthreads();
+    if (warp == 0) {
+        float g[kFeatures];
+        gram_columns<true>(sm, lane, g);
+        chol_lanes(g, lane, sm.diag, sm.inv2);
+        // R2 v = z in lanes 10..12 (R2(i, j) is lane j's g[i]) ...
+        float v[kFeatures];
+#pragma unroll
+        for (int ii = 0; ii < kFeatures; ++ii) {
+            const int i = kFeatures - 1 - ii;
+            float s = g[i];
+#pragma unroll
+            for (int j = i + 1; j < kFeatures; ++j) s = __fmaf_rn(-__shfl_sync(kFull, g[i], j), v[j], s);
+            v[i] = s * sm.inv2[i];
+        }
+        // ... then R1 w = v.
+        float w[kFeatures];
+#pragma unroll
+        for (int ii = 0; ii < kFeatures; ++ii) {
+            const int i = kFeatures - 1 - ii;
+            float s = v[i];
+#pragma unroll
+            for (int j = i + 1; j < kFeatures; ++j) s = __fmaf_rn(-sm.Rm[j][i], w[j], s);
+            w[i] = s * sm.inv1[i];
+        }
+        if (lane >= kFeatures && lane < kFeatures + 3) {
+#pragma unroll
+            for (int k = 0; k < kFeatures; ++k) weights_out[3 * k + (lane - kFeatures)] = w[k];
+        }
+    }
+    __syncthreads();
+}
+
+// METHOD: FitMethod; the binary16 tile (HALF) serves kFitReference only.
+template <bool HALF, int METHOD = kFitReference>
 __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict__ noise, NoiseConst nc,
                                           FitterSmem& sm, float* __restrict__ weights_out,
                                           float* __restrict__ mm_out) {
@@ -521,11 +763,24 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
     for (int f = 0; f < kScaled; ++f) {
         const float bmax = sm.out[f], bmin = sm.out[kScaled + f];
         const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
-        t.set2(kNotScaled + f, 0, scale_by(a01.x, bmin, bmax), scale_by(a01.y, bmin, bmax));
-        t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
+        if constexpr (METHOD == kFitCholQR2 && !HALF) {
+            // Precision form: scale() (bmfr.cl:200-205) by one reciprocal
+            // per column instead of a division per value.
+            const float d = bmax - bmin;
+            const float2 m = dup2(bmin);
+            const float2 y = dup2(fabsf(d) > 1.0f ? __frcp_rn(d) : 1.0f);
+            t.p[kNotScaled + f][0] = mul2(add2(a01, neg2(m)), y);
+            t.p[kNotScaled + f][1] = mul2(add2(a23, neg2(m)), y);
+        } else {
+            t.set2(kNotScaled + f, 0, scale_by(a01.x, bmin, bmax), scale_by(a01.y, bmin, bmax));
+            t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
+        }
     }
 
-    if constexpr (FAST && !HALF) {
+    if constexpr (METHOD == kFitCholQR2 && !HALF) {
+        fit_columns_cqr2(t, noise, nc, sm, weights_out);
+        return;
+    } else if constexpr (METHOD == kFitHouseholder32 && !HALF) {
         fit_columns_fast(t, id, noise, nc, sm);
     } else {
         qr_column<HALF, true>(t, 0, id, noise, nc, sm);

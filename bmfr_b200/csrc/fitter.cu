@@ -29,12 +29,16 @@ struct FitterShared {
     float noise[NOISE_GLOBAL ? 1 : kNoiseTableFloats];
 };
 
-template <bool HALF_TMP, bool ROUND, bool NOISE_GLOBAL>
-__global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
+// METHOD (FitMethod): kFitReference rounds like the reference (a binary16
+// tile when tmp_data is binary16); the precision-form methods need binary16
+// tmp_data and work on a float tile.
+template <bool HALF_TMP, int METHOD, bool NOISE_GLOBAL>
+__global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2)
     k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, float* __restrict__ weights,
              float* __restrict__ mins_maxs, const float* __restrict__ noise_g, int* __restrict__ status) {
     using Shared = FitterShared<HALF_TMP, NOISE_GLOBAL>;
     using TmpT = typename Shared::TmpT;
+    constexpr bool ROUND = HALF_TMP && METHOD == kFitReference;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Shared& S = *reinterpret_cast<Shared*>(smem_raw);
     constexpr uint32_t kTileBytes = kBuffers * kBlockPixels * sizeof(TmpT);
@@ -87,9 +91,8 @@ __global__ void __launch_bounds__(256, (HALF_TMP && ROUND) ? 3 : 2)
             mbar_arrive_expect_tx(&S.bar, kTileBytes);
             bulk_copy_g2s(S.tile, src + (size_t)next * kTileBytes, kTileBytes, &S.bar);
         }
-        // HALF_TMP without ROUND is the precision form (fp32_qr): FP32 QR.
-        fit_block<ROUND, HALF_TMP && !ROUND>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3,
-                                             mins_maxs + (size_t)b * kScaled * 2);
+        fit_block<ROUND, METHOD>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3,
+                                 mins_maxs + (size_t)b * kScaled * 2);
     }
 }
 
@@ -104,10 +107,10 @@ cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <bool HALF_TMP, bool ROUND, bool NOISE_GLOBAL>
+template <bool HALF_TMP, int METHOD, bool NOISE_GLOBAL>
 static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const void* tmp, float* weights,
                                    float* mins_maxs, const float* noise, int* status, cudaStream_t s) {
-    auto kern = k_fitter<HALF_TMP, ROUND, NOISE_GLOBAL>;
+    auto kern = k_fitter<HALF_TMP, METHOD, NOISE_GLOBAL>;
     const int smem = (int)sizeof(FitterShared<HALF_TMP, NOISE_GLOBAL>);
     static int grid_cap[64] = {0};   // per device
     int dev = 0;
@@ -131,20 +134,34 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
 }
 
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                          bool fp32_qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
+                          int qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
                           cudaStream_t s) {
     const int n = g.blocks;
+    // The precision-form methods apply to binary16 tmp_data; float tmp_data
+    // always takes the reference's arithmetic.
+    const int method = half_tmp ? qr : kFitReference;
     if (noise_table) {
-        if (half_tmp && !fp32_qr)
-            return launch_fitter_t<true, true, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
-        if (half_tmp)
-            return launch_fitter_t<true, false, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
-        return launch_fitter_t<false, false, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table, status, s);
+        if (!half_tmp)
+            return launch_fitter_t<false, kFitReference, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table,
+                                                               status, s);
+        if (method == kFitCholQR2)
+            return launch_fitter_t<true, kFitCholQR2, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table,
+                                                            status, s);
+        if (method == kFitHouseholder32)
+            return launch_fitter_t<true, kFitHouseholder32, true>(n, frame, nc, tmp, weights, mins_maxs,
+                                                                  noise_table, status, s);
+        return launch_fitter_t<true, kFitReference, true>(n, frame, nc, tmp, weights, mins_maxs, noise_table,
+                                                          status, s);
     }
-    if (half_tmp && !fp32_qr)
-        return launch_fitter_t<true, true, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
-    if (half_tmp) return launch_fitter_t<true, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
-    return launch_fitter_t<false, false, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
+    if (!half_tmp)
+        return launch_fitter_t<false, kFitReference, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status,
+                                                            s);
+    if (method == kFitCholQR2)
+        return launch_fitter_t<true, kFitCholQR2, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
+    if (method == kFitHouseholder32)
+        return launch_fitter_t<true, kFitHouseholder32, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr,
+                                                               status, s);
+    return launch_fitter_t<true, kFitReference, false>(n, frame, nc, tmp, weights, mins_maxs, nullptr, status, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -181,7 +198,7 @@ static cudaError_t static_scratch_address(void** out) {
 }
 
 cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                                 bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s) {
+                                 int qr, float* weights, float* mins_maxs, cudaStream_t s) {
     void* base = nullptr;
     cudaError_t e = static_scratch_address(&base);
     if (e != cudaSuccess) return e;
@@ -191,7 +208,7 @@ cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, co
     if (e != cudaSuccess) return e;
     e = launch_noise_table(frame, table, s);
     if (e != cudaSuccess) return e;
-    return launch_fitter(g, frame, nc, tmp, half_tmp, fp32_qr, weights, mins_maxs, table, status, s);
+    return launch_fitter(g, frame, nc, tmp, half_tmp, qr, weights, mins_maxs, table, status, s);
 }
 
 }  // namespace bmfr

@@ -18,14 +18,14 @@
 
 namespace bmfr {
 
-template <bool ROUND, bool HALF_TMP, typename HistT>
-__global__ void __launch_bounds__(256, ROUND ? 3 : 2) k_fused_block(BlockJob j) {
+template <int METHOD, bool HALF_TMP, typename HistT>
+__global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2) k_fused_block(BlockJob j) {
     __shared__ FitterSmem sm;
     __shared__ float w_s[kFeatures * 3], mm_s[kScaled * 2];
-    fused_block_body<ROUND, HALF_TMP, HistT>(j, blockIdx.x, sm, w_s, mm_s);
+    fused_block_body<METHOD, HALF_TMP, HistT>(j, blockIdx.x, sm, w_s, mm_s);
 }
 
-template <bool ROUND, bool HALF_TMP, typename HistT>
+template <int METHOD, bool HALF_TMP, typename HistT>
 static cudaError_t launch_fused_t(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
                                   const FusedBuffers& fb, cudaStream_t s) {
     BlockJob j;
@@ -34,21 +34,23 @@ static cudaError_t launch_fused_t(const Geometry& g, const AccumArgs& a, NoiseCo
     j.nc = nc;
     j.second_alpha = second_alpha;
     j.fb = fb;
-    k_fused_block<ROUND, HALF_TMP, HistT><<<g.blocks, kLocal, 0, s>>>(j);
+    k_fused_block<METHOD, HALF_TMP, HistT><<<g.blocks, kLocal, 0, s>>>(j);
     return cudaGetLastError();
 }
 
+template <typename HistT>
+static cudaError_t launch_fused_h(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
+                                  int qr, const FusedBuffers& fb, cudaStream_t s) {
+    if (a.use_half == 0) return launch_fused_t<kFitReference, false, HistT>(g, a, nc, second_alpha, fb, s);
+    if (qr == kFitCholQR2) return launch_fused_t<kFitCholQR2, true, HistT>(g, a, nc, second_alpha, fb, s);
+    if (qr == kFitHouseholder32) return launch_fused_t<kFitHouseholder32, true, HistT>(g, a, nc, second_alpha, fb, s);
+    return launch_fused_t<kFitReference, true, HistT>(g, a, nc, second_alpha, fb, s);
+}
+
 cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
-                               bool fp32_qr, bool half_history, const FusedBuffers& fb, cudaStream_t s) {
-    const bool half_tmp = a.use_half != 0;
-    if (half_history) {
-        if (half_tmp && !fp32_qr) return launch_fused_t<true, true, __half>(g, a, nc, second_alpha, fb, s);
-        if (half_tmp) return launch_fused_t<false, true, __half>(g, a, nc, second_alpha, fb, s);
-        return launch_fused_t<false, false, __half>(g, a, nc, second_alpha, fb, s);
-    }
-    if (half_tmp && !fp32_qr) return launch_fused_t<true, true, float>(g, a, nc, second_alpha, fb, s);
-    if (half_tmp) return launch_fused_t<false, true, float>(g, a, nc, second_alpha, fb, s);
-    return launch_fused_t<false, false, float>(g, a, nc, second_alpha, fb, s);
+                               int qr, bool half_history, const FusedBuffers& fb, cudaStream_t s) {
+    if (half_history) return launch_fused_h<__half>(g, a, nc, second_alpha, qr, fb, s);
+    return launch_fused_h<float>(g, a, nc, second_alpha, qr, fb, s);
 }
 
 }  // namespace bmfr

@@ -23,13 +23,16 @@ __device__ __forceinline__ void tile_set1(Tile<false>& t, int k, int q, float v)
     t.set1(k, q, v);
 }
 
-// ROUND: binary16 tile rounded at every store (reference arithmetic);
-// HALF_TMP: features are rounded to binary16 as the reference's tmp_data
-// stores them (bmfr.cl:471-475); HistT: element type of the colour histories.
-// Block b of job j; ends with every thread past the fit's final barrier.
-template <bool ROUND, bool HALF_TMP, typename HistT>
+// METHOD: FitMethod (the precision-form methods need HALF_TMP); with
+// kFitReference and HALF_TMP the tile is binary16, rounded at every store as
+// the reference rounds; HALF_TMP: features are rounded to binary16 as the
+// reference's tmp_data stores them (bmfr.cl:471-475); HistT: element type of
+// the colour histories.  Block b of job j; ends with every thread past the
+// fit's final barrier.
+template <int METHOD, bool HALF_TMP, typename HistT>
 __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, FitterSmem& sm, float* w_s,
                                                  float* mm_s) {
+    constexpr bool ROUND = HALF_TMP && METHOD == kFitReference;
     const Geometry& g = j.g;
     const AccumArgs& a = j.a;
     const FusedBuffers& fb = j.fb;
@@ -94,7 +97,7 @@ __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, Fitte
     }
 
     // Phase 2: the fit; weights and min/max stay in shared memory.
-    fit_block<ROUND, HALF_TMP && !ROUND>(t, fb.noise, nc, sm, w_s, mm_s);
+    fit_block<ROUND, METHOD>(t, fb.noise, nc, sm, w_s, mm_s);
     if (threadIdx.x < kFeatures * 3) fb.weights[(size_t)b * kFeatures * 3 + threadIdx.x] = w_s[threadIdx.x];
     if (threadIdx.x < kScaled * 2) fb.mins_maxs[(size_t)b * kScaled * 2 + threadIdx.x] = mm_s[threadIdx.x];
 

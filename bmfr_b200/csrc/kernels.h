@@ -21,14 +21,15 @@ cudaError_t launch_fitter_fp64(const Geometry& g, int frame, double noise_amount
 
 // status: device word that receives a nonzero code if a bounded wait ran out.
 // noise_table: the frame's table from launch_noise_table, or null to have
-// every CTA form it in shared memory.
+// every CTA form it in shared memory.  qr: bmfr_params.fp32_qr (0 the
+// reference's arithmetic, 1 CholeskyQR2, 2 Householder in FP32).
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                          bool fp32_qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
+                          int qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
                           cudaStream_t s);
 cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s);
 // The fitter with its scratch in a static device array (no allocation).
 cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
-                                 bool fp32_qr, float* weights, float* mins_maxs, cudaStream_t s);
+                                 int qr, float* weights, float* mins_maxs, cudaStream_t s);
 constexpr size_t kNoiseTableBytes = 9 * 4 * 256 * sizeof(float);
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,
@@ -78,7 +79,7 @@ struct BlockJob {
 };
 
 cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
-                               bool fp32_qr, bool half_history, const FusedBuffers& fb, cudaStream_t s);
+                               int qr, bool half_history, const FusedBuffers& fb, cudaStream_t s);
 
 // NOISE_AMOUNT * 2 split into hi + lo floats.
 inline NoiseConst make_noise_const(double noise_amount) {

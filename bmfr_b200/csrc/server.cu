@@ -59,7 +59,7 @@ struct bmfr_server {
     cudaStream_t stream = nullptr;
 
     std::mutex mu;                       // queues, request states, statistics
-    std::mutex batch_mu;                 // the batch object (steps, stream slots)
+    std::mutex batch_mu;                 // steps and tuning of the batch (its slot table has its own lock)
     std::condition_variable cv_sched;    // work for the scheduler
     std::condition_variable cv_done;     // a request completed
     std::unordered_map<int, std::deque<Request>> pending;   // per open stream
@@ -96,7 +96,9 @@ void schedule_loop(bmfr_server* s) {
         std::vector<Request> take;
         {
             std::unique_lock<std::mutex> lk(s->mu);
+            const int max_in_flight = s->cfg.max_steps_in_flight > 0 ? s->cfg.max_steps_in_flight : 2;
             s->cv_sched.wait(lk, [&] {
+                if (s->steps_outstanding >= max_in_flight) return false;   // requests gather meanwhile
                 if (s->stop) return true;
                 for (auto& kv : s->pending)
                     if (!kv.second.empty()) return true;
@@ -196,6 +198,7 @@ void complete_loop(bmfr_server* s) {
             if (--s->steps_outstanding == 0) s->busy += ms_between(s->busy_since, t);
         }
         s->cv_done.notify_all();
+        s->cv_sched.notify_one();   // room for the next step
     }
 }
 
@@ -220,6 +223,11 @@ int bmfr_server_create(const bmfr_params* params, const bmfr_server_config* conf
     s->cfg = *config;
     cudaGetDevice(&s->device);
     if (int st = bmfr_batch_create(params, config->memory_budget_bytes, &s->batch)) {
+        delete s;
+        return st;
+    }
+    if (int st = bmfr_batch_reserve(s->batch, config->reserve_bytes)) {
+        bmfr_batch_destroy(s->batch);
         delete s;
         return st;
     }
@@ -252,11 +260,9 @@ int bmfr_server_destroy(bmfr_server* s) {
 
 int bmfr_server_open_stream(bmfr_server* s, int width, int height, int* id) {
     if (!s || !id) return fail(BMFR_E_INVALID, "NULL argument");
-    int st;
-    {
-        std::lock_guard<std::mutex> blk(s->batch_mu);
-        st = bmfr_batch_add_stream(s->batch, width, height, s->cfg.own_inputs, id);
-    }
+    // Not under batch_mu: the batch guards its slot table itself, and an
+    // allocation that grows the memory pool must not hold up the steps.
+    const int st = bmfr_batch_add_stream(s->batch, width, height, s->cfg.own_inputs, id);
     std::lock_guard<std::mutex> lk(s->mu);
     if (st == BMFR_E_BUDGET) s->rejected += 1;
     if (st != BMFR_OK) return st;
@@ -276,13 +282,11 @@ int bmfr_server_close_stream(bmfr_server* s, int id) {
         s->open.erase(id);
         s->pending.erase(id);
     }
-    std::lock_guard<std::mutex> blk(s->batch_mu);
     return bmfr_batch_remove_stream(s->batch, id);
 }
 
 int bmfr_server_stream_inputs(bmfr_server* s, int id, bmfr_frame_inputs* in) {
     if (!s) return fail(BMFR_E_INVALID, "server is NULL");
-    std::lock_guard<std::mutex> blk(s->batch_mu);
     return bmfr_batch_stream_inputs(s->batch, id, in);
 }
 

@@ -76,14 +76,21 @@ typedef struct bmfr_params {
                                    binary16; 0: float32                      */
     int compressed_r;              /* 1 (bmfr.cpp:82); accepted, R is internal */
     int cache_tmp_data;            /* 1 (bmfr.cpp:84); 0 is not served         */
-    int fp32_qr;                   /* precision form: 0 rounds every in-place
-                                   tmp update to the tmp type as the reference
-                                   does (bmfr.cl:540, 651); 1 keeps the block
-                                   in fp32 registers through the QR          */
+    int fp32_qr;                   /* the fit's arithmetic (binary16 tmp_data):
+                                   0 the reference's Householder sequence,
+                                   rounding every in-place tmp update to
+                                   binary16 (bmfr.cl:540, 651); precision
+                                   form, the block in FP32 registers:
+                                   1 CholeskyQR2 (BMFR_QR_CHOLESKY2),
+                                   2 the Householder sequence (BMFR_QR_HOUSEHOLDER) */
     int half_history;              /* precision form, plan pipeline only: the
                                    colour histories are stored as binary16   */
     int pipeline;                  /* BMFR_PIPELINE_* for bmfr_denoise_frame   */
 } bmfr_params;
+
+#define BMFR_QR_REFERENCE 0
+#define BMFR_QR_CHOLESKY2 1
+#define BMFR_QR_HOUSEHOLDER 2
 
 /* Sizes derived by bmfr_plan_create (bmfr.cpp:104-118, 315-347). */
 typedef struct bmfr_sizes {

@@ -14,7 +14,11 @@
  * requests arriving while a step is on the GPU join the next one.
  *
  * Conventions as in bmfr_b200.h: status codes, asynchronous calls on a CUDA
- * stream, device pointers unless stated otherwise.
+ * stream, device pointers unless stated otherwise.  Threads: steps, tuning
+ * and autotuning of one batch are called from one thread at a time; streams
+ * may be added, removed and reset from other threads meanwhile (stream
+ * memory comes from a device pool in stream order, so adding or removing a
+ * stream never synchronises the device).
  */
 #ifndef BMFR_BATCH_H
 #define BMFR_BATCH_H
@@ -61,6 +65,10 @@ int bmfr_batch_remove_stream(bmfr_batch* batch, int slot);
 int bmfr_batch_reset_stream(bmfr_batch* batch, int slot);
 int bmfr_batch_stream_frame(const bmfr_batch* batch, int slot);
 size_t bmfr_batch_bytes_in_use(const bmfr_batch* batch);
+/* Grows the batch's device memory pool to hold at least `bytes` (blocking),
+ * so that streams added later take their memory from it without the pool
+ * having to grow while steps run. */
+int bmfr_batch_reserve(bmfr_batch* batch, size_t bytes);
 
 /* Device slots for the stream's next frame (own_inputs streams only). */
 int bmfr_batch_stream_inputs(bmfr_batch* batch, int slot, bmfr_frame_inputs* inputs);
@@ -94,6 +102,9 @@ typedef struct bmfr_server_config {
     size_t memory_budget_bytes;  /* device bytes all streams may hold (0: no limit) */
     int max_streams_per_step;    /* at most this many frames per step (0: every stream that is ready) */
     int own_inputs;              /* streams get input slots (bmfr_server_stream_inputs) */
+    int max_steps_in_flight;     /* steps launched and not finished before the next one is formed
+                                    (0: 2, one running and one queued behind it) */
+    size_t reserve_bytes;        /* stream memory to reserve at creation (bmfr_batch_reserve) */
 } bmfr_server_config;
 
 typedef struct bmfr_server_stats {
@@ -107,8 +118,11 @@ typedef struct bmfr_server_stats {
 } bmfr_server_stats;
 
 /* Starts the server's scheduling thread on the current device.  Requests
- * that arrive while steps are on the GPU are queued and join the next step;
- * each step takes the oldest pending frame of every ready stream. */
+ * that arrive while steps are on the GPU are queued and join the next step,
+ * which is formed once fewer than max_steps_in_flight steps are outstanding;
+ * each step takes the oldest pending frame of every ready stream.  Streams
+ * join and leave without synchronising the device (their memory comes from
+ * a stream-ordered pool). */
 int bmfr_server_create(const bmfr_params* params, const bmfr_server_config* config, bmfr_server** server);
 int bmfr_server_destroy(bmfr_server* server);   /* finishes queued work first */
 

@@ -552,6 +552,34 @@ void orc_fitter(const orc_cfg* cfg, float* weights, float* mins_maxs, void* tmp_
     }
 }
 
+void orc_fitter_matrix(const orc_cfg* cfg, const void* tmp_data, int frame_number, double* out) {
+    Geometry g(cfg);
+    const int nt = threads_of(cfg);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int b = 0; b < g.B; ++b) {
+        std::vector<float> tile(kBuffers * kBlockPixels);
+        load_block(cfg, tmp_data, b, tile.data());
+        double* m = out + (size_t)b * kBuffers * kBlockPixels;
+        for (int i = 0; i < kBuffers * kBlockPixels; ++i) m[i] = tile[i];
+        for (int fb = kNotScaled; fb < kBuffers - 3; ++fb) {
+            double* col = m + fb * kBlockPixels;
+            float bmax = -INFINITY, bmin = INFINITY;
+            for (int i = 0; i < kBlockPixels; ++i) {
+                bmax = fmax_cl((float)col[i], bmax);
+                bmin = fmin_cl((float)col[i], bmin);
+            }
+            for (int i = 0; i < kBlockPixels; ++i) col[i] = scale_d(col[i], bmin, bmax);
+        }
+        for (int fb = 1; fb < kBuffers - 3; ++fb)
+            for (int id = 0; id < kLocal; ++id)
+                for (int q = 0; q < 4; ++q) {
+                    const int idx = id + q * kLocal;
+                    m[fb * kBlockPixels + idx] =
+                        add_random_d(m[fb * kBlockPixels + idx], id, q, fb, frame_number, cfg->noise_amount);
+                }
+    }
+}
+
 void orc_fitter_fp64(const orc_cfg* cfg, double* weights, float* mins_maxs,
                      const void* tmp_data, int frame_number) {
     Geometry g(cfg);

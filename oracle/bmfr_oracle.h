@@ -53,6 +53,12 @@ void orc_fitter(const orc_cfg* cfg, float* weights, float* mins_maxs,
 void orc_fitter_fp64(const orc_cfg* cfg, double* weights, float* mins_maxs,
     const void* tmp_data, int frame_number);
 
+/* The least-squares system every block solves: for each block, its 13
+ * columns of 1024 values after the min/max scaling and the noise of the
+ * first column step, in double precision (out: blocks x 13 x 1024). */
+void orc_fitter_matrix(const orc_cfg* cfg, const void* tmp_data, int frame_number,
+    double* out);
+
 void orc_weighted_sum(const orc_cfg* cfg, const float* weights,
     const float* mins_maxs, float* output, const float* current_normals,
     const float* current_positions, int frame_number);

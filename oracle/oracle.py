@@ -47,10 +47,11 @@ def _load() -> C.CDLL:
     lib.orc_accumulate_noisy_data.argtypes = [C.POINTER(Cfg)] + [vp] * 13 + [C.c_int]
     lib.orc_fitter.argtypes = [C.POINTER(Cfg), vp, vp, vp, C.c_int, C.c_int]
     lib.orc_fitter_fp64.argtypes = [C.POINTER(Cfg), vp, vp, vp, C.c_int]
+    lib.orc_fitter_matrix.argtypes = [C.POINTER(Cfg), vp, C.c_int, vp]
     lib.orc_weighted_sum.argtypes = [C.POINTER(Cfg), vp, vp, vp, vp, vp, C.c_int]
     lib.orc_accumulate_filtered_data.argtypes = [C.POINTER(Cfg)] + [vp] * 8 + [C.c_int]
     lib.orc_taa.argtypes = [C.POINTER(Cfg), vp, vp, vp, vp, C.c_int]
-    for n in ("orc_accumulate_noisy_data", "orc_fitter", "orc_fitter_fp64", "orc_weighted_sum",
+    for n in ("orc_accumulate_noisy_data", "orc_fitter", "orc_fitter_fp64", "orc_fitter_matrix", "orc_weighted_sum",
               "orc_accumulate_filtered_data", "orc_taa", "orc_sizes"):
         getattr(lib, n).restype = None
     return lib
@@ -92,6 +93,12 @@ class Oracle:
 
     def fitter_fp64(self, weights64, mins_maxs, tmp, frame):
         lib.orc_fitter_fp64(C.byref(self.cfg), _p(weights64), _p(mins_maxs), _p(tmp), int(frame))
+
+    def fitter_matrix(self, tmp, frame):
+        """Each block's least-squares system after scaling and noise, float64 (blocks, 13, 1024)."""
+        out = np.empty((self.blocks, 13, 1024), dtype=np.float64)
+        lib.orc_fitter_matrix(C.byref(self.cfg), _p(tmp), int(frame), _p(out))
+        return out
 
     def weighted_sum(self, weights, mins_maxs, out, cur_n, cur_p, frame):
         lib.orc_weighted_sum(C.byref(self.cfg), _p(weights), _p(mins_maxs), _p(out), _p(cur_n), _p(cur_p),

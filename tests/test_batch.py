@@ -48,10 +48,10 @@ def _device_result(ptr, w, h):
     return device_array(ptr, (h, w, 3), np.float32)
 
 
-@pytest.mark.parametrize("precision_form", [True, False])
-def test_batch_equals_streams_alone(cuda, precision_form):
+@pytest.mark.parametrize("qr", [B.QR_REFERENCE, B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
+def test_batch_equals_streams_alone(cuda, qr):
     import torch
-    kw = dict(fp32_qr=1, half_history=1) if precision_form else {}
+    kw = dict(fp32_qr=qr, half_history=1) if qr != B.QR_REFERENCE else {}
     params = B.default_params(pipeline=B.PIPELINE_FUSED, **kw)
     streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
     batch = B.Batch(params)

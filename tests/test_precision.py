@@ -45,13 +45,14 @@ def test_fp64_fitter_matches_oracle(cuda):
     plan.close()
 
 
-def test_fp32_qr_weights_against_fp64(cuda):
+@pytest.mark.parametrize("qr", [B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
+def test_fp32_qr_weights_against_fp64(cuda, qr):
     import torch
     W, H = 256, 192
     sc = B.Scene(17, W, H, 24)
     o = Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared)
     pipe = OraclePipeline(o)
-    plan = B.Plan(W, H, fp32_qr=1)
+    plan = B.Plan(W, H, fp32_qr=qr)
     nb = plan.sizes.blocks
     for f in range(3):
         d = sc.render(f)
@@ -69,15 +70,16 @@ def test_fp32_qr_weights_against_fp64(cuda):
     plan.close()
 
 
+@pytest.mark.parametrize("qr", [B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
-def test_precision_form_output_against_fp64(cuda, pipeline):
+def test_precision_form_output_against_fp64(cuda, pipeline, qr):
     """Binary16 histories + FP32 QR vs the pipeline with the fp64 fitter and
     float histories: mean relative error per frame below 2e-4, at most 0.1 %
     of pixels above 1e-3, no pixel above 2e-2."""
     W, H = 320, 180
     sc = B.Scene(19, W, H, 24)
     ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared), fitter_mode=FITTER_FP64)
-    plan = B.Plan(W, H, fp32_qr=1, half_history=1, pipeline=pipeline,
+    plan = B.Plan(W, H, fp32_qr=qr, half_history=1, pipeline=pipeline,
                   position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
     for f in range(6):
         d = sc.render(f)
