@@ -915,27 +915,30 @@ def main():
     stage_gbs = {k: sb[k] / (v * 1e-3) / 1e9 for k, v in stages.items() if v > 0}
 
     # ---- e2e: host buffers through the C ABI --------------------------------
+    # Uploads, frames and downloads on three streams: the plan orders them,
+    # so frame i+1's upload and frame i-1's download overlap frame i.
     plan.reset()
     out_host = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32).pin_memory()
+    up_stream, down_stream = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
 
     def step_e2e(i):
         f = frame_order(i, nfr)
         pf = frame_order(i - 1, nfr) if i > 0 else f
         plan.upload_frame(host["albedo"][f], host["normals"][f], host["positions"][f], host["noisy"][f],
-                          stream=stream)
+                          stream=up_stream)
         plan.denoise_frame(mats[pf], off, stream=stream)
-        plan.download_result(out_host, stream=stream)
+        plan.download_result(out_host, stream=down_stream)
 
     for i in range(args.warmup):
         step_e2e(i)
-    stream.synchronize()
+    torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_steps = min(args.steps, 120)
-    e0.record(stream)
+    e0.record(up_stream)
     for i in range(args.warmup, args.warmup + e2e_steps):
         step_e2e(i)
-    e1.record(stream)
+    e1.record(down_stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     if pg is not None:

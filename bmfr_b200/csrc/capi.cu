@@ -38,11 +38,14 @@ struct bmfr_plan {
     bmfr::Geometry g;
     int device = 0;
     int frame = 0;
-    // Frame-pipeline buffers (bmfr.cpp:315-347).
-    float* normals[2] = {nullptr, nullptr};
-    float* positions[2] = {nullptr, nullptr};
-    float* albedo = nullptr;
-    float* noisy_in = nullptr;        // this frame's 1-spp colour
+    // Frame-pipeline buffers (bmfr.cpp:315-347).  The plan's input slots
+    // are three sets used in turn (set f % 3 for frame f), so that frame
+    // f+1 can be uploaded while frame f is denoised, which also reads the
+    // normals and positions of frame f-1.
+    float* normals[3] = {nullptr, nullptr, nullptr};
+    float* positions[3] = {nullptr, nullptr, nullptr};
+    float* albedo[3] = {nullptr, nullptr, nullptr};
+    float* noisy_in[3] = {nullptr, nullptr, nullptr};   // the frame's 1-spp colour
     void* noisy_acc[2] = {nullptr, nullptr};    // accumulated noisy history
     uint8_t* spp[2] = {nullptr, nullptr};
     void* tmp = nullptr;
@@ -54,13 +57,18 @@ struct bmfr_plan {
     float* tone_mapped = nullptr;
     void* acc_filt[2] = {nullptr, nullptr};     // accumulated filtered history
     void* result[2] = {nullptr, nullptr};       // TAA history
-    float* result_f32 = nullptr;                // fp32 output when histories are binary16
+    float* result_f32[2] = {nullptr, nullptr};  // fp32 output when histories are binary16
     int* dev_status = nullptr;                  // device error word (bounded waits)
     float* noise_table = nullptr;               // the frame's fitter noise (scratch)
     const float* last_result = nullptr;         // float32 output of the last frame
     bool profiling = false;
     bool profiled_frame = false;
     cudaEvent_t events[6] = {};                 // stage boundaries of the last frame
+    // Ordering of uploads, frames and downloads that run on different
+    // streams: input set k uploaded, frame f done (index f % 3), result of
+    // parity p read back.  The flags say whether the event was recorded.
+    cudaEvent_t ev_uploaded[3] = {}, ev_frame_done[3] = {}, ev_downloaded[2] = {};
+    bool uploaded[3] = {}, downloaded[2] = {}, done_recorded[3] = {};
     std::vector<void*> allocations;
 };
 
@@ -101,6 +109,12 @@ bmfr::AccumArgs accum_args(const bmfr_plan* plan, const float* m, const float* o
 
 void free_plan(bmfr_plan* plan) {
     for (cudaEvent_t& e : plan->events)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : plan->ev_uploaded)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : plan->ev_frame_done)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : plan->ev_downloaded)
         if (e) cudaEventDestroy(e);
     for (void* p : plan->allocations) cudaFree(p);
     delete plan;
@@ -213,20 +227,26 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
         return true;
     };
     bool ok = true;
+    for (int i = 0; i < 3 && ok; ++i)
+        ok = alloc(px * 12, &plan->normals[i]) && alloc(px * 12, &plan->positions[i]) &&
+             alloc(px * 12, &plan->albedo[i]) && alloc(px * 12, &plan->noisy_in[i]);
     for (int i = 0; i < 2 && ok; ++i) {
-        ok = ok && alloc(px * 12, &plan->normals[i]) && alloc(px * 12, &plan->positions[i]) &&
-             alloc(pixel3_bytes(plan, half_hist), &plan->noisy_acc[i]) && alloc(px, &plan->spp[i]) &&
+        ok = ok && alloc(pixel3_bytes(plan, half_hist), &plan->noisy_acc[i]) && alloc(px, &plan->spp[i]) &&
              alloc(pixel3_bytes(plan, half_hist), &plan->acc_filt[i]) &&
              alloc(pixel3_bytes(plan, half_hist), &plan->result[i]);
+        if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32[i]);
     }
-    ok = ok && alloc(px * 12, &plan->albedo) && alloc(px * 12, &plan->noisy_in) &&
-         alloc(tmp_bytes(g, half_tmp), &plan->tmp) &&
+    ok = ok && alloc(tmp_bytes(g, half_tmp), &plan->tmp) &&
          alloc((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &plan->weights) &&
          alloc((size_t)g.blocks * bmfr::kScaled * 2 * 4, &plan->mins_maxs) &&
          alloc(px * 12, &plan->filtered) && alloc(px * 8, &plan->prev_pix) && alloc(px, &plan->accept) &&
          alloc(px * 12, &plan->tone_mapped);
-    if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32);
     if (ok) ok = alloc(sizeof(int), &plan->dev_status) && alloc(bmfr::kNoiseTableBytes, &plan->noise_table);
+    for (int i = 0; i < 3 && ok; ++i)
+        ok = cudaEventCreateWithFlags(&plan->ev_uploaded[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&plan->ev_frame_done[i], cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 2 && ok; ++i)
+        ok = cudaEventCreateWithFlags(&plan->ev_downloaded[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         free_plan(plan);
         return fail(BMFR_E_NOMEM, "device allocation for the plan failed");
@@ -379,11 +399,11 @@ int bmfr_taa(const bmfr_plan* plan, const float* in_prev_frame_pixel, const floa
 
 int bmfr_plan_frame_inputs(bmfr_plan* plan, bmfr_frame_inputs* in) {
     if (!plan || !in) return fail(BMFR_E_INVALID, "NULL argument");
-    const int cur = plan->frame & 1;
-    in->albedo = plan->albedo;
-    in->normals = plan->normals[cur];
-    in->positions = plan->positions[cur];
-    in->noisy = plan->noisy_in;
+    const int k = plan->frame % 3;
+    in->albedo = plan->albedo[k];
+    in->normals = plan->normals[k];
+    in->positions = plan->positions[k];
+    in->noisy = plan->noisy_in[k];
     return BMFR_OK;
 }
 
@@ -393,13 +413,26 @@ int bmfr_plan_upload_frame(bmfr_plan* plan, const float* albedo, const float* no
     if (!albedo || !normals || !positions || !noisy) return fail(BMFR_E_INVALID, "upload: NULL host buffer");
     bmfr_frame_inputs in;
     bmfr_plan_frame_inputs(plan, &in);
+    const int f = plan->frame, k = f % 3;
     const size_t bytes = (size_t)plan->g.W * plan->g.H * 12;
     cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaMemcpyAsync(in.albedo, albedo, bytes, cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaSuccess;
+    // Set k was last read by frame f-2 (its previous normals and positions);
+    // the first two frames (after a reset too) wait for every frame recorded.
+    if (f >= 2) {
+        e = cudaStreamWaitEvent(s, plan->ev_frame_done[(f - 2) % 3], 0);
+    } else {
+        for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+            if (plan->done_recorded[i]) e = cudaStreamWaitEvent(s, plan->ev_frame_done[i], 0);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(in.albedo, albedo, bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(in.normals, normals, bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(in.positions, positions, bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(in.noisy, noisy, bytes, cudaMemcpyHostToDevice, s);
-    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "upload");
+    if (e == cudaSuccess) e = cudaEventRecord(plan->ev_uploaded[k], s);
+    if (e != cudaSuccess) return cuda_fail(e, "upload");
+    plan->uploaded[k] = true;
+    return BMFR_OK;
 }
 
 namespace {
@@ -420,8 +453,20 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     auto mark = [&](int i) {
         if (prof) cudaEventRecord(plan->events[i], s);
     };
+    cudaError_t e = cudaSuccess;
+    // Uploads and downloads may run on other streams: wait for this frame's
+    // input set and for the read-back of the result buffers this frame
+    // overwrites (those of frame f-2).
+    if (plan->uploaded[f % 3] && albedo == plan->albedo[f % 3]) {
+        e = cudaStreamWaitEvent(s, plan->ev_uploaded[f % 3], 0);
+        plan->uploaded[f % 3] = false;
+    }
+    if (e == cudaSuccess && plan->downloaded[cur]) {
+        e = cudaStreamWaitEvent(s, plan->ev_downloaded[cur], 0);
+        plan->downloaded[cur] = false;
+    }
     mark(0);
-    cudaError_t e = bmfr::launch_noise_table(f, plan->noise_table, s);
+    if (e == cudaSuccess) e = bmfr::launch_noise_table(f, plan->noise_table, s);
     bool split = false;
     if (plan->p.pipeline == BMFR_PIPELINE_FUSED) {
         mark(1);
@@ -478,12 +523,14 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     }
     if (!split) mark(3);
     mark(4);
-    float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32 : nullptr);
+    float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
     if (e == cudaSuccess)
         e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped, plan->result[cur],
                              plan->result[prv], f32_out, half_hist, s);
     mark(5);
+    if (e == cudaSuccess) e = cudaEventRecord(plan->ev_frame_done[f % 3], s);
     if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
+    plan->done_recorded[f % 3] = true;
     plan->profiled_frame = prof;
     plan->last_result = half_hist ? f32_out : (const float*)plan->result[cur];
     plan->frame = f + 1;   // swaps every double buffer (bmfr.cpp:482-484)
@@ -496,9 +543,9 @@ int bmfr_denoise_frame(bmfr_plan* plan, const float* prev_frame_camera_matrix, c
                        void* stream) {
     if (int st = check_plan(plan)) return st;
     if (!prev_frame_camera_matrix || !pixel_offset) return fail(BMFR_E_INVALID, "denoise_frame: NULL matrix/offset");
-    const int cur = plan->frame & 1, prv = cur ^ 1;
-    return run_frame(plan, plan->albedo, plan->normals[cur], plan->normals[prv], plan->positions[cur],
-                     plan->positions[prv], plan->noisy_in, nullptr, prev_frame_camera_matrix, pixel_offset,
+    const int k = plan->frame % 3, kp = (plan->frame + 2) % 3;
+    return run_frame(plan, plan->albedo[k], plan->normals[k], plan->normals[kp], plan->positions[k],
+                     plan->positions[kp], plan->noisy_in[k], nullptr, prev_frame_camera_matrix, pixel_offset,
                      (cudaStream_t)stream);
 }
 
@@ -520,14 +567,20 @@ int bmfr_plan_result(const bmfr_plan* plan, const float** result) {
     return BMFR_OK;
 }
 
-int bmfr_plan_download_result(const bmfr_plan* plan, float* host_rgb, void* stream) {
+int bmfr_plan_download_result(bmfr_plan* plan, float* host_rgb, void* stream) {
     if (int st = check_plan(plan)) return st;
     if (!host_rgb) return fail(BMFR_E_INVALID, "download: NULL host buffer");
     const float* r = nullptr;
     if (int st = bmfr_plan_result(plan, &r)) return st;
-    cudaError_t e = cudaMemcpyAsync(host_rgb, r, (size_t)plan->g.W * plan->g.H * 12, cudaMemcpyDeviceToHost,
-                                    (cudaStream_t)stream);
-    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "download");
+    const int f = plan->frame - 1;   // the last denoised frame
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaStreamWaitEvent(s, plan->ev_frame_done[f % 3], 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host_rgb, r, (size_t)plan->g.W * plan->g.H * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(plan->ev_downloaded[f & 1], s);
+    if (e != cudaSuccess) return cuda_fail(e, "download");
+    plan->downloaded[f & 1] = true;
+    return BMFR_OK;
 }
 
 int bmfr_plan_frame_number(const bmfr_plan* plan) { return plan ? plan->frame : BMFR_E_INVALID; }

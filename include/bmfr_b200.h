@@ -223,7 +223,11 @@ typedef struct bmfr_frame_inputs {
 } bmfr_frame_inputs;
 
 int bmfr_plan_frame_inputs(bmfr_plan* plan, bmfr_frame_inputs* inputs);
-/* Host-to-device copies of one frame's four buffers into those slots. */
+/* Host-to-device copies of one frame's four buffers into those slots.
+ * Uploads, bmfr_denoise_frame and bmfr_plan_download_result may be called on
+ * three different streams: the plan keeps three input sets and two result
+ * buffers and orders them with events, so that the upload of frame f+1 and
+ * the download of frame f-1 overlap the denoising of frame f. */
 int bmfr_plan_upload_frame(bmfr_plan* plan, const float* albedo,
                            const float* normals, const float* positions,
                            const float* noisy, void* stream);
@@ -255,7 +259,9 @@ int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io,
 
 /* Device pointer of the last finished frame's TAA output (W*H*3 floats). */
 int bmfr_plan_result(const bmfr_plan* plan, const float** result);
-int bmfr_plan_download_result(const bmfr_plan* plan, float* host_rgb, void* stream);
+/* Device-to-host copy of the last finished frame's output; ordered after
+ * that frame on any stream, and before the frame that reuses its buffer. */
+int bmfr_plan_download_result(bmfr_plan* plan, float* host_rgb, void* stream);
 int bmfr_plan_frame_number(const bmfr_plan* plan);
 int bmfr_plan_reset(bmfr_plan* plan);   /* frame counter back to 0 */
 

@@ -80,3 +80,39 @@ def test_pipeline_rejects_bad_arguments(cuda):
     with pytest.raises(ValueError):
         plan.denoise_frame(np.zeros(15), np.zeros(2))
     plan.close()
+
+
+@pytest.mark.parametrize("half_history", [0, 1])
+def test_three_stream_frame_loop(cuda, half_history):
+    """Uploads, frames and downloads issued on three streams, each frame's
+    upload and the previous frame's download overlapping the denoising: the
+    plan's own ordering must give every frame exactly the output of the
+    one-stream loop."""
+    import torch
+    W, H, frames = 160, 96, 7
+    sc = B.Scene(23, W, H, 10)
+    data = [sc.render(f) for f in range(frames)]
+    pin = lambda a: torch.from_numpy(a).pin_memory()
+    host = [{k: pin(d[k]) for k in ("albedo", "normals", "positions", "noisy")} for d in data]
+    kw = dict(half_history=half_history, fp32_qr=1 if half_history else 0,
+              position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
+    one = B.Plan(W, H, **kw)
+    want = []
+    for f in range(frames):
+        h = host[f]
+        one.upload_frame(h["albedo"], h["normals"], h["positions"], h["noisy"])
+        one.denoise_frame(sc.prev_camera(f), sc.pixel_offset(f))
+        want.append(one.download_result())
+    three = B.Plan(W, H, **kw)
+    up, comp, down = (torch.cuda.Stream(device=cuda) for _ in range(3))
+    outs = [torch.empty((H, W, 3), dtype=torch.float32).pin_memory() for _ in range(frames)]
+    for f in range(frames):
+        h = host[f]
+        three.upload_frame(h["albedo"], h["normals"], h["positions"], h["noisy"], stream=up)
+        three.denoise_frame(sc.prev_camera(f), sc.pixel_offset(f), stream=comp)
+        three.download_result(outs[f], stream=down)
+    torch.cuda.synchronize()
+    for f in range(frames):
+        np.testing.assert_array_equal(outs[f].numpy(), want[f], err_msg=f"frame {f}")
+    one.close()
+    three.close()
