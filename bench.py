@@ -62,7 +62,9 @@ def stage_bytes(w, h):
         "fitter": 26 * Pm + 168 * B,
         "weighted_sum": 36 * P,
         "accumulate_filtered_data": 70 * P,
-        "weighted_sum+accumulate_filtered_data": 82 * P,
+        # one pass: N, P, prev_pix, accept, albedo, spp, acc_prev read; filtered,
+        # acc_cur, tone_mapped written (float histories)
+        "weighted_sum+accumulate_filtered_data": 94 * P,
         "taa": 44 * P,
         "noise_table": 9 * 4 * 256 * 4,
         # accumulate (95 B/px + 26 B read per margin pixel from the inputs, no
@@ -144,16 +146,18 @@ def cpu_port_frames_per_s(w, h, frames, sc, budget_s=12.0, min_frames=3, threads
     # Frame 0 has no history; time frames 1.. as the reference's stats do.
     d = frames[0]
     pipe.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(0), sc.pixel_offset(0))
-    n, t0 = 0, time.perf_counter()
+    n, t0, stage_s = 0, time.perf_counter(), {}
     while n < len(frames) - 1:
         f = n + 1
         d = frames[f]
         pipe.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f), sc.pixel_offset(f))
+        for k, v in pipe.stage_seconds.items():
+            stage_s[k] = stage_s.get(k, 0.0) + v
         n += 1
         if n >= min_frames and time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return n / dt, n, dt
+    return n / dt, n, dt, {k: 1e3 * v / n for k, v in stage_s.items()}
 
 
 def run_reference(args, world, rank):
@@ -169,11 +173,14 @@ def run_reference(args, world, rank):
         f = frame_order(i, nf)
         d = frames[f]
         pipe.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f), sc.pixel_offset(f))
+    stage_s = {}
     t0 = time.perf_counter()
     for i in range(args.warmup, args.warmup + args.steps):
         f = frame_order(i, nf)
         d = frames[f]
         pipe.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f), sc.pixel_offset(f))
+        for k, v in pipe.stage_seconds.items():
+            stage_s[k] = stage_s.get(k, 0.0) + v
     dt = time.perf_counter() - t0
     v = args.steps / dt
     sample = f"{args.steps} full 1280x720 frames of the oracle pipeline (5 stages), OpenMP over {cores} threads"
@@ -185,6 +192,7 @@ def run_reference(args, world, rank):
                    "height": HEIGHT, "frames": FRAMES, "parallelism": "host cores"},
         "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "stages_ms": {k: 1e3 * v / args.steps for k, v in stage_s.items()},
         "note": "the reference's OpenCL kernels have no runnable platform on this box; this is the oracle port",
     }), flush=True)
 
@@ -807,6 +815,52 @@ def run_precision(args, world, rank, local, dev, barrier, pg):
         }), flush=True)
 
 
+def dropin_stage_ms(B, torch, dev, stream, params, frames, mats, off, nframes):
+    """Each of the five drop-in stage entry points (the reference's kernels,
+    opencl/bmfr.cl) timed alone with events around its call, on the same
+    frames, buffers allocated by the caller as in opencl/bmfr.cpp:315-347."""
+    plan = B.Plan(WIDTH, HEIGHT, params=params)
+    px = WIDTH * HEIGHT
+    z = lambda n, dt=torch.float32: torch.zeros(n, dtype=dt, device=dev)
+    noisy, acc, res = [z(px * 3), z(px * 3)], [z(px * 3), z(px * 3)], [z(px * 3), z(px * 3)]
+    spp = [z(px, torch.uint8), z(px, torch.uint8)]
+    prev_pix, accept = z(px * 2), z(px, torch.uint8)
+    tmp = z(plan.sizes.tmp_data_bytes, torch.uint8)
+    nb = plan.sizes.blocks
+    w, mm, filt, tone = z(nb * 30), z(nb * 12), z(px * 3), z(px * 3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    names = ("accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa")
+    out = {k: [] for k in names}
+    nfr = frames["albedo"].shape[0]
+    with torch.cuda.stream(stream):
+        for i in range(nframes + 3):
+            f = frame_order(i, nfr)
+            pf = frame_order(i - 1, nfr) if i > 0 else f
+            c, q = i & 1, (i & 1) ^ 1
+            noisy[c].copy_(frames["noisy"][f].reshape(-1))
+            ev[0].record(stream)
+            B.accumulate_noisy_data(plan, prev_pix, accept, frames["normals"][f], frames["normals"][pf],
+                                    frames["positions"][f], frames["positions"][pf], noisy[c], noisy[q], spp[q],
+                                    spp[c], tmp, mats[pf], off, i, stream=stream)
+            ev[1].record(stream)
+            B.fitter(plan, w, mm, tmp, i, stream=stream)
+            ev[2].record(stream)
+            B.weighted_sum(plan, w, mm, filt, frames["normals"][f], frames["positions"][f], noisy[c], i,
+                           stream=stream)
+            ev[3].record(stream)
+            B.accumulate_filtered_data(plan, filt, prev_pix, accept, frames["albedo"][f], tone, spp[c], acc[q],
+                                       acc[c], i, stream=stream)
+            ev[4].record(stream)
+            B.taa(plan, prev_pix, tone, res[c], res[q], i, stream=stream)
+            ev[5].record(stream)
+            ev[5].synchronize()
+            if i >= 3:
+                for k, n in enumerate(names):
+                    out[n].append(ev[k].elapsed_time(ev[k + 1]))
+    plan.close()
+    return {k: float(np.mean(v)) for k, v in out.items()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -913,6 +967,7 @@ def main():
                 "frac": achieved / hbm_peak, "peak_source": peak_kind, "bytes_per_launch": sb[dominant],
                 "traffic": None}
     stage_gbs = {k: sb[k] / (v * 1e-3) / 1e9 for k, v in stages.items() if v > 0}
+    dropin = dropin_stage_ms(B, torch, dev, stream, plan.params, devf, mats, off, min(args.steps, 30))
 
     # ---- e2e: host buffers through the C ABI --------------------------------
     # Uploads, frames and downloads on three streams: the plan orders them,
@@ -950,9 +1005,10 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        fps, n, dt = cpu_port_frames_per_s(WIDTH, HEIGHT, frames, sc)
+        fps, n, dt, cpu_stages = cpu_port_frames_per_s(WIDTH, HEIGHT, frames, sc)
         cpu = {"value": fps, "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{n} consecutive 1280x720 frames of the oracle pipeline ({dt:.1f} s)"}
+               "sample": f"{n} consecutive 1280x720 frames of the oracle pipeline ({dt:.1f} s)",
+               "stages_ms": cpu_stages}
 
     plan.close()
     if rank == 0:
@@ -965,6 +1021,8 @@ def main():
                        "tmp_data": "binary16", "parallelism": f"replicas x{world}",
                        "l2": "no flush: per-frame working set ~180 MB (inputs + histories) exceeds the 126 MB L2"},
             "stages_ms": stages, "stages_gbs": stage_gbs,
+            "dropin_stages_ms": dropin,
+            "dropin_stages_gbs": {k: sb[k] / (v * 1e-3) / 1e9 for k, v in dropin.items() if v > 0},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks.summary(), "gpu_launches": launches_per_frame * args.steps,
         }

@@ -187,12 +187,12 @@ class Plan:
     def enable_profiling(self, enable: bool = True) -> None:
         check(lib.bmfr_plan_enable_profiling(self.handle, int(enable)), "bmfr_plan_enable_profiling")
 
-    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa")
+    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data", None, "taa")
     FUSED_STAGES = ("noise_table", "block_kernel", None, None, "taa")
 
     def stage_times(self) -> dict:
         """Milliseconds per kernel of the last profiled frame (the staged
-        pipeline's five stages, or the fused pipeline's three kernels)."""
+        pipeline's four kernels, or the fused pipeline's three)."""
         ms = (C.c_float * 5)()
         check(lib.bmfr_plan_stage_times(self.handle, ms), "bmfr_plan_stage_times")
         names = self.FUSED_STAGES if self.params.pipeline == PIPELINE_FUSED else self.STAGES
@@ -399,7 +399,7 @@ class Batch:
         check(lib.bmfr_batch_get_tuning(self.handle, C.byref(t)), "bmfr_batch_get_tuning")
         return t
 
-    def set_tuning(self, block_ctas_per_sm=0, taa_tile_w=32, taa_tile_h=8, staging_depth=0) -> None:
+    def set_tuning(self, block_ctas_per_sm=0, taa_tile_w=30, taa_tile_h=32, staging_depth=0) -> None:
         t = BatchTuning(block_ctas_per_sm, taa_tile_w, taa_tile_h, staging_depth)
         check(lib.bmfr_batch_set_tuning(self.handle, C.byref(t)), "bmfr_batch_set_tuning")
 

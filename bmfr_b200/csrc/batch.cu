@@ -107,22 +107,19 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
     }
 }
 
-template <int TW, int TH, typename HistT>
-__global__ void __launch_bounds__(TW* TH) k_batch_taa(const BatchStepDesc* __restrict__ d) {
+// TAA tiles of 30 columns x 4R rows: four warps per CTA, R rows each
+// (taa_strip).
+template <int R, typename HistT>
+__global__ void __launch_bounds__(128) k_batch_taa(const BatchStepDesc* __restrict__ d) {
     const int nt = d->n_tiles;
     for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
         const int s = stream_of_tile(d, tile);
         const BatchStreamJob& J = d->s[s];
-        const Geometry& g = J.job.g;
         const int t = tile - J.tile_start;
-        const int px = (t % J.tiles_x) * TW + (int)(threadIdx.x % TW);
-        const int py = (t / J.tiles_x) * TH + (int)(threadIdx.x / TW);
-        if (px >= g.W || py >= g.H) continue;
-        const int lp = py * g.W + px;
-        const float3 r = taa_px(g, J.job.a.frame, J.taa_alpha, px, py, J.job.fb.prev_pix[lp], J.job.fb.tone_mapped,
-                                (const HistT*)J.result_prev);
-        hist_store((HistT*)J.result_hist, lp, r);
-        if (J.result_out) store3(J.result_out, lp, r);
+        taa_strip<R, HistT>(J.job.g, J.job.a.frame, J.taa_alpha, (t % J.tiles_x) * 30,
+                            (t / J.tiles_x) * 4 * R + (int)(threadIdx.x >> 5) * R, J.job.fb.prev_pix,
+                            J.job.fb.tone_mapped, (const HistT*)J.result_prev, (HistT*)J.result_hist,
+                            J.result_out);
     }
 }
 
@@ -180,20 +177,19 @@ int batch_block_occupancy(int qr, bool half_tmp, bool half_history) {
     return dispatch_blocks<float>(qr, half_tmp, Occupancy{});
 }
 
-template <int TW, int TH>
+template <int R>
 static cudaError_t launch_taa_t(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
-    const int grid = sms * (2048 / (TW * TH));
-    if (half_history) k_batch_taa<TW, TH, __half><<<grid, TW * TH, 0, s>>>(desc);
-    else k_batch_taa<TW, TH, float><<<grid, TW * TH, 0, s>>>(desc);
+    const int grid = sms * 16;
+    if (half_history) k_batch_taa<R, __half><<<grid, 128, 0, s>>>(desc);
+    else k_batch_taa<R, float><<<grid, 128, 0, s>>>(desc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const BatchTuning& t, int sms,
                              cudaStream_t s) {
-    if (t.tile_w == 32 && t.tile_h == 4) return launch_taa_t<32, 4>(desc, half_history, sms, s);
-    if (t.tile_w == 64 && t.tile_h == 4) return launch_taa_t<64, 4>(desc, half_history, sms, s);
-    if (t.tile_w == 16 && t.tile_h == 16) return launch_taa_t<16, 16>(desc, half_history, sms, s);
-    return launch_taa_t<32, 8>(desc, half_history, sms, s);
+    if (t.tile_h == 16) return launch_taa_t<4>(desc, half_history, sms, s);
+    if (t.tile_h == 64) return launch_taa_t<16>(desc, half_history, sms, s);
+    return launch_taa_t<8>(desc, half_history, sms, s);
 }
 
 }  // namespace bmfr

@@ -97,7 +97,7 @@ struct bmfr_batch {
     int sms = 0;
     size_t budget = 0, used = 0;
     std::vector<StreamSlot> slots = std::vector<StreamSlot>(BMFR_BATCH_MAX_STREAMS);
-    bmfr::BatchTuning tuning{0, 32, 8, 0};
+    bmfr::BatchTuning tuning{0, 30, 32, 0};
     int block_occupancy = 1;
     bmfr::BatchStepDesc* d_desc = nullptr;
     bmfr::BatchStepDesc* h_desc[2] = {nullptr, nullptr};
@@ -500,10 +500,8 @@ int bmfr_batch_get_tuning(const bmfr_batch* b, bmfr_batch_tuning* t) {
 int bmfr_batch_set_tuning(bmfr_batch* b, const bmfr_batch_tuning* t) {
     if (int st = check_batch(b)) return st;
     if (!t) return fail(BMFR_E_INVALID, "tuning is NULL");
-    const bool shape_ok = (t->taa_tile_w == 32 && (t->taa_tile_h == 8 || t->taa_tile_h == 4)) ||
-                          (t->taa_tile_w == 64 && t->taa_tile_h == 4) ||
-                          (t->taa_tile_w == 16 && t->taa_tile_h == 16);
-    if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 32x8, 32x4, 64x4 or 16x16");
+    const bool shape_ok = t->taa_tile_w == 30 && (t->taa_tile_h == 16 || t->taa_tile_h == 32 || t->taa_tile_h == 64);
+    if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 30x16, 30x32 or 30x64");
     if (t->block_ctas_per_sm < 0 || t->staging_depth < 0 || t->staging_depth > 4)
         return fail(BMFR_E_INVALID, "bad block CTAs per SM or staging depth");
     b->tuning.block_ctas_per_sm = t->block_ctas_per_sm;
@@ -534,13 +532,13 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
         *ms /= steps;
         return BMFR_OK;
     };
-    bmfr_batch_tuning best{0, 32, 8, 0};
+    bmfr_batch_tuning best{0, 30, 32, 0};
     float best_t = 1e30f;
     int status = BMFR_OK;
     // Blocks per SM and staging depth together, then the TAA CTA shape.
     for (int ctas = 1; ctas <= b->block_occupancy && status == BMFR_OK; ++ctas) {
         for (int depth = 0; depth <= 2 && status == BMFR_OK; ++depth) {
-            bmfr_batch_tuning t{ctas, 32, 8, depth};
+            bmfr_batch_tuning t{ctas, 30, 32, depth};
             float ms = 0.f;
             status = time_tuning(t, &ms);
             if (status == BMFR_OK && ms < best_t) {
@@ -549,8 +547,8 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
             }
         }
     }
-    const int shapes[3][2] = {{32, 4}, {64, 4}, {16, 16}};
-    for (int i = 0; i < 3 && status == BMFR_OK; ++i) {
+    const int shapes[2][2] = {{30, 16}, {30, 64}};
+    for (int i = 0; i < 2 && status == BMFR_OK; ++i) {
         bmfr_batch_tuning t = best;
         t.taa_tile_w = shapes[i][0];
         t.taa_tile_h = shapes[i][1];

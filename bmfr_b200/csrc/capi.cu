@@ -467,7 +467,6 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     }
     mark(0);
     if (e == cudaSuccess) e = bmfr::launch_noise_table(f, plan->noise_table, s);
-    bool split = false;
     if (plan->p.pipeline == BMFR_PIPELINE_FUSED) {
         mark(1);
         bmfr::FusedBuffers fb;
@@ -504,24 +503,15 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
                                     plan->p.fp32_qr, plan->weights, plan->mins_maxs, plan->noise_table,
                                     plan->dev_status, s);
         mark(2);
-        if (!half_hist) {
-            split = true;
-            if (e == cudaSuccess)
-                e = bmfr::launch_weighted_sum(g, f, plan->weights, plan->mins_maxs, plan->filtered, cur_n, cur_p, s);
-            mark(3);
-            if (e == cudaSuccess)
-                e = bmfr::launch_accumulate_filtered(g, f, plan->p.second_blend_alpha, plan->filtered,
-                                                     plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
-                                                     plan->spp[cur], (const float*)plan->acc_filt[prv],
-                                                     (float*)plan->acc_filt[cur], s);
-        } else if (e == cudaSuccess) {
+        // weighted_sum and accumulate_filtered_data in one pass per pixel
+        // (the filtered colour is still written for inspection).
+        if (e == cudaSuccess)
             e = bmfr::launch_weighted_sum_accumulate(g, f, plan->p.second_blend_alpha, plan->weights,
                                                      plan->mins_maxs, cur_n, cur_p, plan->filtered, plan->prev_pix,
                                                      plan->accept, albedo, plan->tone_mapped, plan->spp[cur],
-                                                     plan->acc_filt[prv], plan->acc_filt[cur], true, s);
-        }
+                                                     plan->acc_filt[prv], plan->acc_filt[cur], half_hist, s);
     }
-    if (!split) mark(3);
+    mark(3);
     mark(4);
     float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
     if (e == cudaSuccess)

@@ -182,38 +182,21 @@ __device__ __forceinline__ float3 accumulate_filtered_px(const Geometry& g, int 
 }
 
 // taa body (bmfr.cl:873-973).
+// YCoCg of one colour, unnormalised (bmfr.cl:184-198).
+__device__ __forceinline__ void rgb_to_ycocg(float3 s, float (&ycc)[3]) {
+    ycc[0] = (s.x * 1.0f + s.y * 2.0f) + s.z * 1.0f;
+    ycc[1] = (s.x * 2.0f + s.y * 0.0f) + s.z * -2.0f;
+    ycc[2] = (s.x * -1.0f + s.y * 2.0f) + s.z * -1.0f;
+}
+
+// The second half of taa (bmfr.cl:904-973) for pixel (px, py) whose
+// tonemapped colour is `mine`, given the YCoCg bounds of its 3x3 box and
+// its cross: history bilinear, clamp, blend.
 template <typename HistT>
-__device__ __forceinline__ float3 taa_px(const Geometry& g, int frame, float taa_alpha, int px, int py,
-                                         float2 pp, const float* __restrict__ new_frame,
-                                         const HistT* __restrict__ prev_frame) {
-    const int lp = py * g.W + px;
-    const float3 mine = load3(new_frame, lp);
-    const int ix = floor_to_int(pp.x), iy = floor_to_int(pp.y);
-    if (frame == 0 || ix < -1 || iy < -1 || ix >= g.W || iy >= g.H) return mine;
-    float mnb[3] = {INFINITY, INFINITY, INFINITY}, mnc[3] = {INFINITY, INFINITY, INFINITY};
-    float mxb[3] = {-INFINITY, -INFINITY, -INFINITY}, mxc[3] = {-INFINITY, -INFINITY, -INFINITY};
-#pragma unroll
-    for (int y = -1; y < 2; ++y) {
-#pragma unroll
-        for (int x = -1; x < 2; ++x) {
-            const int sx = px + x, sy = py + y;
-            if (sx >= 0 && sy >= 0 && sx < g.W && sy < g.H) {
-                const float3 s = (x == 0 && y == 0) ? mine : load3(new_frame, sy * g.W + sx);
-                const float ycc[3] = {(s.x * 1.0f + s.y * 2.0f) + s.z * 1.0f,
-                                      (s.x * 2.0f + s.y * 0.0f) + s.z * -2.0f,
-                                      (s.x * -1.0f + s.y * 2.0f) + s.z * -1.0f};
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (x == 0 || y == 0) {
-                        mnc[c] = fmin_cl(mnc[c], ycc[c]);
-                        mxc[c] = fmax_cl(mxc[c], ycc[c]);
-                    }
-                    mnb[c] = fmin_cl(mnb[c], ycc[c]);
-                    mxb[c] = fmax_cl(mxb[c], ycc[c]);
-                }
-            }
-        }
-    }
+__device__ __forceinline__ float3 taa_finish(const Geometry& g, float taa_alpha, float2 pp, int ix, int iy,
+                                             float3 mine, const float (&mnb)[3], const float (&mxb)[3],
+                                             const float (&mnc)[3], const float (&mxc)[3],
+                                             const HistT* __restrict__ prev_frame) {
     float3 prev = make_float3(0.f, 0.f, 0.f);
     float total = 0.0f;
     const float fx = pp.x - (float)ix, fy = pp.y - (float)iy;
@@ -236,9 +219,8 @@ __device__ __forceinline__ float3 taa_px(const Geometry& g, int frame, float taa
     prev.x = prev.x / total;
     prev.y = prev.y / total;
     prev.z = prev.z / total;
-    const float pyc[3] = {(prev.x * 1.0f + prev.y * 2.0f) + prev.z * 1.0f,
-                          (prev.x * 2.0f + prev.y * 0.0f) + prev.z * -2.0f,
-                          (prev.x * -1.0f + prev.y * 2.0f) + prev.z * -1.0f};
+    float pyc[3];
+    rgb_to_ycocg(prev, pyc);
     float cl[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -253,5 +235,121 @@ __device__ __forceinline__ float3 taa_px(const Geometry& g, int frame, float taa
     return make_float3(taa_alpha * mine.x + om * rgb.x, taa_alpha * mine.y + om * rgb.y,
                        taa_alpha * mine.z + om * rgb.z);
 }
+
+// taa (bmfr.cl:868-973) of pixel (px, py) whose tonemapped colour is `mine`;
+// nb(x, y, ycc) gives the YCoCg of the in-image neighbour (px+x, py+y).
+template <typename HistT, typename Nb>
+__device__ __forceinline__ float3 taa_core(const Geometry& g, int frame, float taa_alpha, int px, int py, float2 pp,
+                                           float3 mine, Nb&& nb, const HistT* __restrict__ prev_frame) {
+    const int ix = floor_to_int(pp.x), iy = floor_to_int(pp.y);
+    if (frame == 0 || ix < -1 || iy < -1 || ix >= g.W || iy >= g.H) return mine;
+    float mnb[3] = {INFINITY, INFINITY, INFINITY}, mnc[3] = {INFINITY, INFINITY, INFINITY};
+    float mxb[3] = {-INFINITY, -INFINITY, -INFINITY}, mxc[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+    for (int y = -1; y < 2; ++y) {
+#pragma unroll
+        for (int x = -1; x < 2; ++x) {
+            const int sx = px + x, sy = py + y;
+            if (sx >= 0 && sy >= 0 && sx < g.W && sy < g.H) {
+                float ycc[3];
+                nb(x, y, ycc);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (x == 0 || y == 0) {
+                        mnc[c] = fmin_cl(mnc[c], ycc[c]);
+                        mxc[c] = fmax_cl(mxc[c], ycc[c]);
+                    }
+                    mnb[c] = fmin_cl(mnb[c], ycc[c]);
+                    mxb[c] = fmax_cl(mxb[c], ycc[c]);
+                }
+            }
+        }
+    }
+    return taa_finish(g, taa_alpha, pp, ix, iy, mine, mnb, mxb, mnc, mxc, prev_frame);
+}
+
+// taa over a strip of R rows per thread.  A warp covers 30 image columns
+// x0..x0+29 in lanes 1..30 (lanes 0 and 31 hold the halo columns) and walks
+// rows y0..y0+R-1: each thread reads and converts one pixel per row (R+2
+// rows with the halo), takes its left and right neighbours by shuffles, and
+// keeps a three-row window of horizontal minima and maxima, so a pixel's
+// nine neighbours cost about one load and one YCoCg conversion.  Neighbours
+// outside the image or NaN enter as +-inf, which the reference's fmin/fmax
+// ignore in the same way (bmfr.cl:884-902; fmin_cl keeps its first operand
+// on a NaN), so the bounds equal the reference's up to the sign of a zero
+// bound.
+template <int R, typename HistT>
+__device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float taa_alpha, int x0, int y0,
+                                          const float2* __restrict__ prev_pix, const float* __restrict__ new_frame,
+                                          const HistT* __restrict__ prev_frame, HistT* __restrict__ result_hist,
+                                          float* __restrict__ result_out) {
+    const int lane = threadIdx.x & 31;
+    const int x = x0 - 1 + lane;
+    const bool col_in = x >= 0 && x < g.W;
+    const bool writer = lane >= 1 && lane <= 30 && col_in;
+    float3 rgb[3];
+    float cmn[3][3], cmx[3][3], hmn[3][3], hmx[3][3];   // [window row][channel]
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r) {
+        const int k = r % 3;
+        const int y = y0 - 1 + r;
+        const bool in = col_in && y >= 0 && y < g.H;
+        const float3 s = in ? load3(new_frame, y * g.W + x) : make_float3(0.f, 0.f, 0.f);
+        rgb[k] = s;
+        float ycc[3];
+        rgb_to_ycocg(s, ycc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const bool ok = in && ycc[c] == ycc[c];
+            const float vmn = ok ? ycc[c] : INFINITY, vmx = ok ? ycc[c] : -INFINITY;
+            cmn[k][c] = vmn;
+            cmx[k][c] = vmx;
+            const float l = __shfl_up_sync(0xffffffffu, ycc[c], 1), rr = __shfl_down_sync(0xffffffffu, ycc[c], 1);
+            const unsigned okm = __ballot_sync(0xffffffffu, ok);
+            const bool lok = lane > 0 && ((okm >> (lane - 1)) & 1u);
+            const bool rok = lane < 31 && ((okm >> (lane + 1)) & 1u);
+            hmn[k][c] = fminf(fminf(lok ? l : INFINITY, vmn), rok ? rr : INFINITY);
+            hmx[k][c] = fmaxf(fmaxf(lok ? l : -INFINITY, vmx), rok ? rr : -INFINITY);
+        }
+        if (r >= 2) {
+            const int up = (r - 2) % 3, mid = (r - 1) % 3, dn = k;
+            const int py = y0 + r - 2;
+            if (writer && py < g.H) {
+                const int lp = py * g.W + x;
+                const float2 pp = prev_pix[lp];
+                const float3 mine = rgb[mid];
+                const int ix = floor_to_int(pp.x), iy = floor_to_int(pp.y);
+                float3 out = mine;
+                if (!(frame == 0 || ix < -1 || iy < -1 || ix >= g.W || iy >= g.H)) {
+                    float mnb[3], mxb[3], mnc[3], mxc[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        mnb[c] = fminf(fminf(hmn[up][c], hmn[mid][c]), hmn[dn][c]);
+                        mxb[c] = fmaxf(fmaxf(hmx[up][c], hmx[mid][c]), hmx[dn][c]);
+                        mnc[c] = fminf(fminf(cmn[up][c], hmn[mid][c]), cmn[dn][c]);
+                        mxc[c] = fmaxf(fmaxf(cmx[up][c], hmx[mid][c]), cmx[dn][c]);
+                    }
+                    out = taa_finish(g, taa_alpha, pp, ix, iy, mine, mnb, mxb, mnc, mxc, prev_frame);
+                }
+                hist_store(result_hist, lp, out);
+                if (result_out) store3(result_out, lp, out);
+            }
+        }
+    }
+}
+
+// taa of one pixel, neighbours read from global memory.
+template <typename HistT>
+__device__ __forceinline__ float3 taa_px(const Geometry& g, int frame, float taa_alpha, int px, int py,
+                                         float2 pp, const float* __restrict__ new_frame,
+                                         const HistT* __restrict__ prev_frame) {
+    const float3 mine = load3(new_frame, py * g.W + px);
+    auto nb = [&](int x, int y, float (&ycc)[3]) {
+        const float3 s = (x == 0 && y == 0) ? mine : load3(new_frame, (py + y) * g.W + px + x);
+        rgb_to_ycocg(s, ycc);
+    };
+    return taa_core(g, frame, taa_alpha, px, py, pp, mine, nb, prev_frame);
+}
+
 
 }  // namespace bmfr

@@ -121,19 +121,17 @@ __global__ void __launch_bounds__(256) k_weighted_sum_accumulate(
     store3(tone_mapped, lp, tm);
 }
 
+constexpr int kTaaRows = 8;
+
 template <typename HistT>
-__global__ void __launch_bounds__(256) k_taa(Geometry g, int frame, float taa_alpha,
+__global__ void __launch_bounds__(128) k_taa(Geometry g, int frame, float taa_alpha,
                                              const float2* __restrict__ prev_pix,
                                              const float* __restrict__ new_frame,
                                              HistT* __restrict__ result,
                                              const HistT* __restrict__ prev_frame,
                                              float* __restrict__ result_f32) {
-    const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
-    if (px >= g.W || py >= g.H) return;
-    const int lp = py * g.W + px;
-    const float3 r = taa_px(g, frame, taa_alpha, px, py, prev_pix[lp], new_frame, prev_frame);
-    hist_store(result, lp, r);
-    if (result_f32) store3(result_f32, lp, r);
+    taa_strip<kTaaRows, HistT>(g, frame, taa_alpha, blockIdx.x * 30, (blockIdx.y * 4 + (threadIdx.x >> 5)) * kTaaRows,
+                               prev_pix, new_frame, prev_frame, result, result_f32);
 }
 
 // ---------------------------------------------------------------------------
@@ -142,6 +140,8 @@ __global__ void __launch_bounds__(256) k_taa(Geometry g, int frame, float taa_al
 
 static dim3 margin_grid(const Geometry& g) { return dim3(g.MW / 32, g.MH / 8); }
 static dim3 image_grid(const Geometry& g) { return dim3((g.W + 31) / 32, (g.H + 7) / 8); }
+// TAA: 128-thread CTAs of four warps, each warp 30 columns x kTaaRows rows.
+static dim3 taa_grid(const Geometry& g) { return dim3((g.W + 29) / 30, (g.H + 4 * kTaaRows - 1) / (4 * kTaaRows)); }
 
 cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float2* prev_pix, uint8_t* accept,
                                     const float* cur_n, const float* prev_n, const float* cur_p,
@@ -206,11 +206,11 @@ cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const floa
                        const float* new_frame, void* result, const void* prev_frame, float* result_f32,
                        bool half_history, cudaStream_t s) {
     if (half_history)
-        k_taa<__half><<<image_grid(g), dim3(32, 8), 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
+        k_taa<__half><<<taa_grid(g), 128, 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
                                                            (__half*)result, (const __half*)prev_frame,
                                                            result_f32);
     else
-        k_taa<float><<<image_grid(g), dim3(32, 8), 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
+        k_taa<float><<<taa_grid(g), 128, 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
                                                           (float*)result, (const float*)prev_frame,
                                                           result_f32);
     return cudaGetLastError();

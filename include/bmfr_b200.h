@@ -283,9 +283,11 @@ int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
  * enabled, every denoise call records CUDA events between its stages.
  * bmfr_plan_stage_times waits for the last frame and returns milliseconds of
  * the staged pipeline's [accumulate_noisy_data (with the frame's fitter
- * noise table), fitter, weighted_sum, accumulate_filtered_data, taa].  The
- * fused pipeline reports [noise table, block kernel (accumulate, fitter,
- * weighted sum and filtered accumulation), 0, 0, taa]. */
+ * noise table), fitter, weighted_sum + accumulate_filtered_data (one kernel
+ * in the plan pipeline), 0, taa].  The fused pipeline reports [noise table,
+ * block kernel (accumulate, fitter, weighted sum and filtered accumulation),
+ * 0, 0, taa].  The five drop-in stage entry points time separately with
+ * events around each call. */
 #define BMFR_STAGE_COUNT 5
 int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable);
 int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);

@@ -39,7 +39,7 @@ typedef struct bmfr_batch bmfr_batch;
 /* Launch parameters of a step, chosen by bmfr_batch_autotune. */
 typedef struct bmfr_batch_tuning {
     int block_ctas_per_sm;  /* persistent CTAs of the block kernel per SM (0: as many as fit) */
-    int taa_tile_w;         /* TAA CTA shape: 32x8, 32x4, 64x4 or 16x16 */
+    int taa_tile_w;         /* TAA CTA tile: 30 columns x 16, 32 or 64 rows */
     int taa_tile_h;
     int staging_depth;      /* 0: blocks from an atomic queue; k > 0: static order with the
                                inputs of each CTA's next k blocks prefetched into L2 */

@@ -10,6 +10,7 @@ so this oracle is checked only against hand-derived known-answer tests.
 from __future__ import annotations
 
 import ctypes as C
+import time
 import subprocess
 from pathlib import Path
 
@@ -117,6 +118,8 @@ class OraclePipeline:
     """The reference host program's frame loop (opencl/bmfr.cpp:417-485) over
     the oracle kernels, with the six double buffers swapped every frame."""
 
+    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum", "accumulate_filtered_data", "taa")
+
     def __init__(self, oracle: Oracle, fitter_mode=FITTER_REFERENCE):
         self.o = oracle
         self.mode = fitter_mode
@@ -140,15 +143,26 @@ class OraclePipeline:
         self.positions[c][...] = positions
         self.noisy[c][...] = noisy
         o = self.o
+        t = [time.perf_counter()]
         o.accumulate_noisy_data(self.prev_pix, self.accept, self.normals[c], self.normals[p], self.positions[c],
                                 self.positions[p], self.noisy[c], self.noisy[p], self.spp[p], self.spp[c],
                                 self.tmp, matrix, offset, f)
+        t.append(time.perf_counter())
         self.tmp_after_accumulate = self.tmp.copy()
+        t.append(time.perf_counter())
         o.fitter(self.weights, self.mins_maxs, self.tmp, f, self.mode)
+        t.append(time.perf_counter())
         o.weighted_sum(self.weights, self.mins_maxs, self.filtered, self.normals[c], self.positions[c], f)
+        t.append(time.perf_counter())
         alb = np.ascontiguousarray(albedo, dtype=np.float32)
         o.accumulate_filtered_data(self.filtered, self.prev_pix, self.accept, alb, self.tone_mapped, self.spp[c],
                                    self.acc[p], self.acc[c], f)
+        t.append(time.perf_counter())
         o.taa(self.prev_pix, self.tone_mapped, self.result[c], self.result[p], f)
+        t.append(time.perf_counter())
+        # Seconds per stage of this frame (the reference's per-kernel
+        # profile, opencl/bmfr.cpp:488-517); the copy of tmp_data is left out.
+        self.stage_seconds = dict(zip(self.STAGES, (t[1] - t[0], t[3] - t[2], t[4] - t[3], t[5] - t[4],
+                                                    t[6] - t[5])))
         self.frame = f + 1
         return self.result[c]
