@@ -384,41 +384,51 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
 // Sum over the CTA of v[0..15] (any order); result k in sm.out[k].  A
 // transposing butterfly leaves each lane pair with one value summed over
 // the warp; eight warps then meet in shared memory.
-__device__ __forceinline__ void block_sum16(float (&v)[16], FitterSmem& sm) {
+template <bool MAX>
+__device__ __forceinline__ float op16(float a, float b) {
+    return MAX ? fmaxf(a, b) : a + b;
+}
+
+// op16<MAX> over the CTA of v[0..15]: sums (MAX = false) or maxima.
+template <bool MAX>
+__device__ __forceinline__ void block_reduce16(float (&v)[16], FitterSmem& sm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const bool up = lane & 16;
         const float send = up ? v[k] : v[k + 8], keep = up ? v[k + 8] : v[k];
-        v[k] = keep + __shfl_xor_sync(kFull, send, 16);
+        v[k] = op16<MAX>(keep, __shfl_xor_sync(kFull, send, 16));
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const bool up = lane & 8;
         const float send = up ? v[k] : v[k + 4], keep = up ? v[k + 4] : v[k];
-        v[k] = keep + __shfl_xor_sync(kFull, send, 8);
+        v[k] = op16<MAX>(keep, __shfl_xor_sync(kFull, send, 8));
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const bool up = lane & 4;
         const float send = up ? v[k] : v[k + 2], keep = up ? v[k + 2] : v[k];
-        v[k] = keep + __shfl_xor_sync(kFull, send, 4);
+        v[k] = op16<MAX>(keep, __shfl_xor_sync(kFull, send, 4));
     }
     {
         const bool up = lane & 2;
         const float send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
-        v[0] = keep + __shfl_xor_sync(kFull, send, 2);
+        v[0] = op16<MAX>(keep, __shfl_xor_sync(kFull, send, 2));
     }
-    v[0] = v[0] + __shfl_xor_sync(kFull, v[0], 1);
+    v[0] = op16<MAX>(v[0], __shfl_xor_sync(kFull, v[0], 1));
     const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
     if ((lane & 1) == 0) sm.part[idx * 8 + warp] = v[0];
     __syncthreads();
     if (threadIdx.x < 16) {
         const float* p = sm.part + threadIdx.x * 8;
-        sm.out[threadIdx.x] = ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
+        sm.out[threadIdx.x] = op16<MAX>(op16<MAX>(op16<MAX>(p[0], p[1]), op16<MAX>(p[2], p[3])),
+                                        op16<MAX>(op16<MAX>(p[4], p[5]), op16<MAX>(p[6], p[7])));
     }
     __syncthreads();
 }
+
+__device__ __forceinline__ void block_sum16(float (&v)[16], FitterSmem& sm) { block_reduce16<false>(v, sm); }
 
 // Partial sums of column COL, held in tile column COL: v[0] the norm of
 // rows >= COL+1, v[1+i] the Gram sum of rows >= COL with column COL+1+i.
@@ -739,50 +749,76 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
                                           FitterSmem& sm, float* __restrict__ weights_out,
                                           float* __restrict__ mm_out) {
     const int id = work_item_id();
-    // Min/max scaling of features 4..9 (bmfr.cl:511-542).
-    float mm[12];
+    if constexpr (METHOD != kFitReference && !HALF) {
+        // Precision form: the twelve minima and maxima in one transposing
+        // butterfly (minima as maxima of the negated values); min and max
+        // are exact in any order, so only the sign of a zero bound can
+        // differ from the reference's tree.
+        float v[16];
 #pragma unroll
-    for (int f = 0; f < kScaled; ++f) {
-        const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
-        const float a[4] = {a01.x, a01.y, a23.x, a23.y};
-        float mx = -INFINITY, mn = INFINITY;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            mx = fmax_cl(a[q], mx);
-            mn = fmin_cl(a[q], mn);
+        for (int f = 0; f < kScaled; ++f) {
+            const float2 a01 = t.p[kNotScaled + f][0], a23 = t.p[kNotScaled + f][1];
+            v[f] = fmaxf(fmaxf(a01.x, a01.y), fmaxf(a23.x, a23.y));
+            v[kScaled + f] = fmaxf(fmaxf(-a01.x, -a01.y), fmaxf(-a23.x, -a23.y));
         }
-        mm[f] = mx;
-        mm[kScaled + f] = mn;
-    }
-    block_reduce<12, 2, 1>(mm, 12, kScaled, sm);
-    if (threadIdx.x < 2 * kScaled) {
-        const int f = threadIdx.x >> 1;
-        mm_out[threadIdx.x] = (threadIdx.x & 1) ? sm.out[f] : sm.out[kScaled + f];
-    }
 #pragma unroll
-    for (int f = 0; f < kScaled; ++f) {
-        const float bmax = sm.out[f], bmin = sm.out[kScaled + f];
-        const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
-        if constexpr (METHOD == kFitCholQR2 && !HALF) {
-            // Precision form: scale() (bmfr.cl:200-205) by one reciprocal
-            // per column instead of a division per value.
+        for (int k = 2 * kScaled; k < 16; ++k) v[k] = -INFINITY;
+        block_reduce16<true>(v, sm);
+        if (threadIdx.x < 2 * kScaled) {
+            const int f = threadIdx.x >> 1;
+            mm_out[threadIdx.x] = (threadIdx.x & 1) ? sm.out[f] : -sm.out[kScaled + f];
+        }
+#pragma unroll
+        for (int f = 0; f < kScaled; ++f) {
+            const float bmax = sm.out[f], bmin = -sm.out[kScaled + f];
             const float d = bmax - bmin;
             const float2 m = dup2(bmin);
-            const float2 y = dup2(fabsf(d) > 1.0f ? __frcp_rn(d) : 1.0f);
-            t.p[kNotScaled + f][0] = mul2(add2(a01, neg2(m)), y);
-            t.p[kNotScaled + f][1] = mul2(add2(a23, neg2(m)), y);
+            if constexpr (METHOD == kFitCholQR2) {
+                // scale() (bmfr.cl:200-205) by one reciprocal per column.
+                const float2 y = dup2(fabsf(d) > 1.0f ? __frcp_rn(d) : 1.0f);
+                t.p[kNotScaled + f][0] = mul2(add2(t.p[kNotScaled + f][0], neg2(m)), y);
+                t.p[kNotScaled + f][1] = mul2(add2(t.p[kNotScaled + f][1], neg2(m)), y);
+            } else {
+                const float2 a01 = t.p[kNotScaled + f][0], a23 = t.p[kNotScaled + f][1];
+                t.set2(kNotScaled + f, 0, scale_by(a01.x, bmin, bmax), scale_by(a01.y, bmin, bmax));
+                t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
+            }
+        }
+        if constexpr (METHOD == kFitCholQR2) {
+            fit_columns_cqr2(t, noise, nc, sm, weights_out);
+            return;
         } else {
+            fit_columns_fast(t, id, noise, nc, sm);
+        }
+    } else {
+        // Min/max scaling of features 4..9 (bmfr.cl:511-542), the
+        // reference's reduction tree.
+        float mm[12];
+#pragma unroll
+        for (int f = 0; f < kScaled; ++f) {
+            const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
+            const float a[4] = {a01.x, a01.y, a23.x, a23.y};
+            float mx = -INFINITY, mn = INFINITY;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                mx = fmax_cl(a[q], mx);
+                mn = fmin_cl(a[q], mn);
+            }
+            mm[f] = mx;
+            mm[kScaled + f] = mn;
+        }
+        block_reduce<12, 2, 1>(mm, 12, kScaled, sm);
+        if (threadIdx.x < 2 * kScaled) {
+            const int f = threadIdx.x >> 1;
+            mm_out[threadIdx.x] = (threadIdx.x & 1) ? sm.out[f] : sm.out[kScaled + f];
+        }
+#pragma unroll
+        for (int f = 0; f < kScaled; ++f) {
+            const float bmax = sm.out[f], bmin = sm.out[kScaled + f];
+            const float2 a01 = t.get2(kNotScaled + f, 0), a23 = t.get2(kNotScaled + f, 1);
             t.set2(kNotScaled + f, 0, scale_by(a01.x, bmin, bmax), scale_by(a01.y, bmin, bmax));
             t.set2(kNotScaled + f, 1, scale_by(a23.x, bmin, bmax), scale_by(a23.y, bmin, bmax));
         }
-    }
-
-    if constexpr (METHOD == kFitCholQR2 && !HALF) {
-        fit_columns_cqr2(t, noise, nc, sm, weights_out);
-        return;
-    } else if constexpr (METHOD == kFitHouseholder32 && !HALF) {
-        fit_columns_fast(t, id, noise, nc, sm);
-    } else {
         qr_column<HALF, true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1
         for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);

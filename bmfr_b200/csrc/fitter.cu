@@ -1,16 +1,28 @@
 // fitter.cu — standalone fitter kernel (opencl/bmfr.cl:490-700).
 //
 // Persistent CTAs of 256 threads, as many as fit on the SMs.  Each CTA walks
-// blocks b = blockIdx.x, + gridDim.x, ...: the block's 13 x 1024 tmp_data
-// values arrive by one bulk TMA copy (contiguous 26 KB, no tensor map
-// needed) into shared memory, move to registers, and the copy of the CTA's
-// next block is issued at once so that it overlaps the fit.
+// blocks b = blockIdx.x, + gridDim.x, ...: a block's 13 x 1024 tmp_data
+// values arrive in shared memory by one TMA copy and move to registers, and
+// the copy of a later block is issued at once so that it overlaps the fit.
+//
+// Binary16 tmp_data comes in as a 2-D tensor copy (rows of 64 halves, 208
+// rows per block) with the 128-byte swizzle: the eight lanes of a warp that
+// read one 16-byte chunk of a row meet three other lane groups at rows
+// 64 halves apart, which without the swizzle fall in the same four banks
+// (four-way conflicts on every load); the swizzle spreads them over 16
+// banks.  With the frame's noise table in global memory the CTA keeps two
+// tile buffers, so the copy of the block after next is in flight while the
+// current one is fitted.  Float tmp_data uses a one-dimensional bulk copy.
 //
 // The feature-noise table of the frame is either formed by each CTA in its
 // shared memory (the drop-in entry point: no scratch memory, so calls on
 // different streams never share state) or read from a table that an earlier
 // kernel of the frame pipeline wrote to global memory (smaller CTAs, more of
 // them per SM).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
 #include <mutex>
 #include <type_traits>
 
@@ -20,77 +32,105 @@
 
 namespace bmfr {
 
+constexpr int kTileRows = kBuffers * kBlockPixels / 64;   // 208 rows of 64 halves per block
+
 template <bool HALF_TMP, bool NOISE_GLOBAL>
 struct FitterShared {
     using TmpT = typename std::conditional<HALF_TMP, __half, float>::type;
-    alignas(128) TmpT tile[kBuffers * kBlockPixels];
+    static constexpr int kStages = (HALF_TMP && NOISE_GLOBAL) ? 2 : 1;
+    alignas(1024) TmpT tile[kStages][kBuffers * kBlockPixels];
     FitterSmem sm;
-    alignas(8) uint64_t bar;
+    alignas(8) uint64_t bar[kStages];
     float noise[NOISE_GLOBAL ? 1 : kNoiseTableFloats];
 };
+
+// Byte offset of half h of a block tile copied with the 128-byte swizzle:
+// row h / 64, 16-byte chunk (h % 64) / 8 XOR the row's low three bits.
+__device__ __forceinline__ uint32_t swizzled_half(uint32_t h) {
+    const uint32_t r = h >> 6, c = h & 63u;
+    return (r << 7) | ((((c >> 3) ^ r) & 7u) << 4) | ((c & 7u) << 1);
+}
 
 // METHOD (FitMethod): kFitReference rounds like the reference (a binary16
 // tile when tmp_data is binary16); the precision-form methods need binary16
 // tmp_data and work on a float tile.
 template <bool HALF_TMP, int METHOD, bool NOISE_GLOBAL>
 __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2)
-    k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, float* __restrict__ weights,
-             float* __restrict__ mins_maxs, const float* __restrict__ noise_g, int* __restrict__ status) {
+    k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, const __grid_constant__ CUtensorMap tmap,
+             float* __restrict__ weights, float* __restrict__ mins_maxs, const float* __restrict__ noise_g,
+             int* __restrict__ status) {
     using Shared = FitterShared<HALF_TMP, NOISE_GLOBAL>;
     using TmpT = typename Shared::TmpT;
+    constexpr int kStages = Shared::kStages;
     constexpr bool ROUND = HALF_TMP && METHOD == kFitReference;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    Shared& S = *reinterpret_cast<Shared*>(smem_raw);
+    extern __shared__ unsigned char smem_raw[];
+    // The swizzled copy needs a 1024-byte aligned destination.
+    Shared& S = *reinterpret_cast<Shared*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     constexpr uint32_t kTileBytes = kBuffers * kBlockPixels * sizeof(TmpT);
     const char* src = static_cast<const char*>(tmp);
     const int id = work_item_id();
+    auto issue = [&](int stage, int blk) {
+        mbar_arrive_expect_tx(&S.bar[stage], kTileBytes);
+        if constexpr (HALF_TMP) tensor_copy_2d_g2s(S.tile[stage], &tmap, 0, blk * kTileRows, &S.bar[stage]);
+        else bulk_copy_g2s(S.tile[stage], src + (size_t)blk * kTileBytes, kTileBytes, &S.bar[stage]);
+    };
 
-    int b = blockIdx.x;
     if (threadIdx.x == 0) {
-        mbar_init(&S.bar, 1);
+        for (int st = 0; st < kStages; ++st) mbar_init(&S.bar[st], 1);
         fence_barrier_init();
         S.sm.status = 0;
-        if (b < nblocks) {
-            mbar_arrive_expect_tx(&S.bar, kTileBytes);
-            bulk_copy_g2s(S.tile, src + (size_t)b * kTileBytes, kTileBytes, &S.bar);
-        }
+        for (int st = 0; st < kStages; ++st)
+            if (blockIdx.x + st * (int)gridDim.x < nblocks) issue(st, blockIdx.x + st * gridDim.x);
     }
     if (!NOISE_GLOBAL) fill_noise_table(S.noise, frame);
     const float* noise = NOISE_GLOBAL ? noise_g : S.noise;
     __syncthreads();
 
-    uint32_t phase = 0;
-    for (; b < nblocks; b += gridDim.x, phase ^= 1u) {
-        if (threadIdx.x == 0 && !mbar_wait_bounded(&S.bar, phase)) S.sm.status = kDevTimeout;
+    int it = 0;
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x, ++it) {
+        const int st = it % kStages;
+        const uint32_t phase = (uint32_t)(it / kStages) & 1u;
+        if (threadIdx.x == 0 && !mbar_wait_bounded(&S.bar[st], phase)) S.sm.status = kDevTimeout;
         __syncthreads();
         if (S.sm.status) {
             if (threadIdx.x == 0) {
                 atomicExch(status, kDevTimeout);
-                mbar_wait_bounded(&S.bar, phase);   // let the copy in flight land
+                // let the copies in flight land
+                for (int k = 0; k < kStages; ++k)
+                    if (b + k * (int)gridDim.x < nblocks) mbar_wait_bounded(&S.bar[(it + k) % kStages], (uint32_t)((it + k) / kStages) & 1u);
             }
             return;
         }
         Tile<ROUND> t;
+        const TmpT* tile = S.tile[st];
+        // Row k*16 + 4q + id/64 of the tile holds (k, q); its swizzle XOR
+        // (low three row bits) does not depend on k.
+        uint32_t qoff[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) qoff[q] = swizzled_half((uint32_t)(q * kLocal + id));
 #pragma unroll
         for (int k = 0; k < kBuffers; ++k) {
-            const TmpT* col = S.tile + k * kBlockPixels + id;
-            if constexpr (ROUND) {
-                t.h[k][0] = __halves2half2(col[0], col[kLocal]);
-                t.h[k][1] = __halves2half2(col[2 * kLocal], col[3 * kLocal]);
-            } else {
+            if constexpr (HALF_TMP) {
+                const unsigned char* base = reinterpret_cast<const unsigned char*>(tile) + k * kBlockPixels * 2;
+                __half v[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if constexpr (HALF_TMP) t.set1(k, q, __half2float(col[q * kLocal]));
-                    else t.set1(k, q, col[q * kLocal]);
+                for (int q = 0; q < 4; ++q) v[q] = *reinterpret_cast<const __half*>(base + qoff[q]);
+                if constexpr (ROUND) {
+                    t.h[k][0] = __halves2half2(v[0], v[1]);
+                    t.h[k][1] = __halves2half2(v[2], v[3]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) t.set1(k, q, __half2float(v[q]));
                 }
+            } else {
+                const TmpT* col = tile + k * kBlockPixels + id;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) t.set1(k, q, col[q * kLocal]);
             }
         }
         __syncthreads();   // the buffer is free again
-        const int next = b + gridDim.x;
-        if (threadIdx.x == 0 && next < nblocks) {
-            mbar_arrive_expect_tx(&S.bar, kTileBytes);
-            bulk_copy_g2s(S.tile, src + (size_t)next * kTileBytes, kTileBytes, &S.bar);
-        }
+        const int next = b + kStages * (int)gridDim.x;
+        if (threadIdx.x == 0 && next < nblocks) issue(st, next);
         fit_block<ROUND, METHOD>(t, noise, nc, S.sm, weights + (size_t)b * kFeatures * 3,
                                  mins_maxs + (size_t)b * kScaled * 2);
     }
@@ -107,11 +147,40 @@ cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// binary16 tmp_data of `nblocks` blocks as rows of 64 halves; one box is
+// one block (208 rows), swizzled by 128 bytes.
+static cudaError_t encode_tmp_map(const void* tmp, int nblocks, CUtensorMap* map) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[2] = {64, (cuuint64_t)nblocks * kTileRows};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {64, (cuuint32_t)kTileRows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(tmp), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 template <bool HALF_TMP, int METHOD, bool NOISE_GLOBAL>
 static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const void* tmp, float* weights,
                                    float* mins_maxs, const float* noise, int* status, cudaStream_t s) {
     auto kern = k_fitter<HALF_TMP, METHOD, NOISE_GLOBAL>;
-    const int smem = (int)sizeof(FitterShared<HALF_TMP, NOISE_GLOBAL>);
+    const int smem = (int)sizeof(FitterShared<HALF_TMP, NOISE_GLOBAL>) + 1024;   // + alignment slack
     static int grid_cap[64] = {0};   // per device
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -129,7 +198,13 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
     }
     const int grid = nblocks < grid_cap[dev] ? nblocks : grid_cap[dev];
     if (grid <= 0) return cudaSuccess;
-    kern<<<grid, kLocal, smem, s>>>(nblocks, frame, nc, tmp, weights, mins_maxs, noise, status);
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof map);
+    if (HALF_TMP) {
+        e = encode_tmp_map(tmp, nblocks, &map);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid, kLocal, smem, s>>>(nblocks, frame, nc, tmp, map, weights, mins_maxs, noise, status);
     return cudaGetLastError();
 }
 
