@@ -230,7 +230,8 @@ def run_batched(args, world, rank, local, dev, barrier, pg):
         frames.append(fl)
     stream.synchronize()
     n = len(scenes)
-    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    pipeline = B.PIPELINE_FUSED if args.pipeline == "fused" else B.PIPELINE_STAGED
+    params = B.default_params(pipeline=pipeline, fp32_qr=1, half_history=1)
     batch = B.Batch(params)
     slots = [batch.add_stream(sc.width, sc.height) for sc in scenes]
 
@@ -304,7 +305,7 @@ def run_batched(args, world, rank, local, dev, barrier, pg):
             "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered, 30 frames per stream)",
-            "config": {"workload": "batched form, 24 streams", "streams": len(BATCH_STREAMS),
+            "config": {"workload": "batched form, 24 streams", "streams": len(BATCH_STREAMS), "pipeline": args.pipeline,
                        "pixels_per_step": pixels, "frames": nfr, "tuning": {
                            "block_ctas_per_sm": tuning.block_ctas_per_sm, "taa_tile": [tuning.taa_tile_w, tuning.taa_tile_h],
                            "staging_depth": tuning.staging_depth}, "tuned_ms_per_step": tuned_ms},
@@ -393,7 +394,8 @@ def run_served(args, world, rank, local, dev, barrier, pg):
                                          p["positions"]), sc.camera(pf), sc.pixel_offset(f), d, p))
         pools.append({"w": w, "h": h, "sc": sc, "frames": fr, "tab": tab})
     stream.synchronize()
-    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1,
+    params = B.default_params(pipeline=B.PIPELINE_FUSED if args.pipeline == "fused" else B.PIPELINE_STAGED,
+                              fp32_qr=1, half_history=1,
                               position_limit_squared=pools[0]["sc"].position_limit_squared,
                               normal_limit_squared=pools[0]["sc"].normal_limit_squared)
     seconds = float(args.seconds)
@@ -638,7 +640,7 @@ def run_served(args, world, rank, local, dev, barrier, pg):
             "warmup": 0, "ms_per_step": 1e3 * st["busy_seconds"] / max(st["steps"], 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered frame pools)",
-            "config": {"workload": "served form, 64 Poisson streams", "seats": SERVED_SEATS,
+            "config": {"workload": "served form, 64 Poisson streams", "seats": SERVED_SEATS, "pipeline": args.pipeline,
                        "mix": [[w, h, p] for (w, h), p in SERVED_MIX], "rates_hz": [30, 60],
                        "mean_lifetime_frames": SERVED_LIFETIME, "budget_bytes": SERVED_BUDGET,
                        "trace_seconds": seconds, "warm_seconds": warm_s, "requests_after_warmup": n_req,

@@ -39,6 +39,7 @@ struct StreamSlot {
     float* weights = nullptr;
     float* mins_maxs = nullptr;
     float* noise = nullptr;
+    void* tmp = nullptr;   // staged pipeline: the stream's tmp_data
     // own input slots
     float* normals[2] = {nullptr, nullptr};
     float* positions[2] = {nullptr, nullptr};
@@ -70,6 +71,8 @@ size_t carve(StreamSlot& s, const bmfr_params& p, int w, int h, bool own_inputs,
     take((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &s.weights);
     take((size_t)g.blocks * bmfr::kScaled * 2 * 4, &s.mins_maxs);
     take(bmfr::kNoiseTableBytes, &s.noise);
+    if (p.pipeline == BMFR_PIPELINE_STAGED)
+        take((size_t)g.MW * g.MH * bmfr::kBuffers * (p.use_half_precision_in_tmp_data ? 2 : 4), &s.tmp);
     if (own_inputs) {
         for (int i = 0; i < 2; ++i) {
             take(px * 12, &s.normals[i]);
@@ -170,9 +173,14 @@ int build_graphs(bmfr_batch* b) {
         e = cudaMemcpyAsync(b->d_desc, b->h_desc[k], sizeof(bmfr::BatchStepDesc), cudaMemcpyHostToDevice, cs);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(int), cs);
         if (e == cudaSuccess) e = bmfr::launch_batch_noise(b->d_desc, BMFR_BATCH_MAX_STREAMS, cs);
-        if (e == cudaSuccess)
+        if (b->p.pipeline == BMFR_PIPELINE_STAGED) {
+            if (e == cudaSuccess) e = bmfr::launch_batch_accumulate(b->d_desc, b->p.half_history != 0, b->sms, cs);
+            if (e == cudaSuccess) e = bmfr::launch_batch_fitter(b->d_desc, b->p.fp32_qr, half_tmp, ctas * b->sms, cs);
+            if (e == cudaSuccess) e = bmfr::launch_batch_wsacc(b->d_desc, b->p.half_history != 0, b->sms, cs);
+        } else if (e == cudaSuccess) {
             e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr, half_tmp,
                                           b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms, cs);
+        }
         if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
         if (e == cudaSuccess) e = e2;
@@ -205,7 +213,7 @@ bmfr::AccumArgs step_args(const bmfr_batch* b, const float* m, const float* off,
 int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, const bmfr_frame_io* io,
               const float* matrices, const float* offsets) {
     const int tw = b->tuning.tile_w, th = b->tuning.tile_h;
-    int blocks = 0, tiles = 0;
+    int blocks = 0, tiles = 0, acc_tiles = 0, px_tiles = 0;
     for (int i = 0; i < n; ++i) {
         StreamSlot& s = b->slots[slots[i]];
         const int f = s.frame, cur = f & 1, prv = cur ^ 1;
@@ -250,9 +258,16 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
         J.result_hist = s.result[cur];
         J.result_prev = s.result[prv];
         J.result_out = (fi && fi->result) ? fi->result : s.result_f32;
+        J.tmp = s.tmp;
+        J.acc_tile_start = acc_tiles;
+        J.px_tile_start = px_tiles;
         blocks += s.g.blocks;
         tiles += J.tiles_x * ((s.height + th - 1) / th);
+        acc_tiles += (s.g.MW / 32) * (s.g.MH / 8);
+        px_tiles += ((s.width + 31) / 32) * ((s.height + 7) / 8);
     }
+    d->n_acc_tiles = acc_tiles;
+    d->n_px_tiles = px_tiles;
     d->n_streams = n;
     d->n_blocks = blocks;
     d->n_tiles = tiles;
@@ -275,6 +290,8 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
     *out = nullptr;
     if (!params->cache_tmp_data) return fail(BMFR_E_UNSUPPORTED, "cache_tmp_data = 0 is not served");
     if (params->fp32_qr < 0 || params->fp32_qr > 2) return fail(BMFR_E_INVALID, "fp32_qr must be 0, 1 or 2");
+    if (params->pipeline != BMFR_PIPELINE_STAGED && params->pipeline != BMFR_PIPELINE_FUSED)
+        return fail(BMFR_E_INVALID, "unknown pipeline");
     int dev = -1;
     if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess) {
         cudaGetLastError();
@@ -282,13 +299,14 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
     }
     bmfr_batch* b = new bmfr_batch;
     b->p = *params;
-    b->p.pipeline = BMFR_PIPELINE_FUSED;
     b->device = dev;
     b->budget = memory_budget_bytes;
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-    b->block_occupancy = std::max(1, bmfr::batch_block_occupancy(params->fp32_qr,
-                                                                 params->use_half_precision_in_tmp_data != 0,
-                                                                 params->half_history != 0));
+    const bool half_tmp = params->use_half_precision_in_tmp_data != 0;
+    b->block_occupancy =
+        std::max(1, params->pipeline == BMFR_PIPELINE_STAGED
+                        ? bmfr::batch_fitter_occupancy(params->fp32_qr, half_tmp)
+                        : bmfr::batch_block_occupancy(params->fp32_qr, half_tmp, params->half_history != 0));
     cudaError_t e = cudaMalloc(&b->d_desc, sizeof(bmfr::BatchStepDesc));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * sizeof(int));
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
@@ -537,7 +555,8 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
     int status = BMFR_OK;
     // Blocks per SM and staging depth together, then the TAA CTA shape.
     for (int ctas = 1; ctas <= b->block_occupancy && status == BMFR_OK; ++ctas) {
-        for (int depth = 0; depth <= 2 && status == BMFR_OK; ++depth) {
+        const int max_depth = b->p.pipeline == BMFR_PIPELINE_STAGED ? 0 : 2;   // staging: fused step only
+        for (int depth = 0; depth <= max_depth && status == BMFR_OK; ++depth) {
             bmfr_batch_tuning t{ctas, 30, 32, depth};
             float ms = 0.f;
             status = time_tuning(t, &ms);

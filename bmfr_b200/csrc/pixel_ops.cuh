@@ -108,6 +108,36 @@ __device__ __forceinline__ void store_tmp_row(const Geometry& g, void* tmp, bool
     for (int k = 0; k < kBuffers; ++k) store_feature(tmp, base + (size_t)k * kBlockPixels, f[k], half_tmp);
 }
 
+// accumulate_noisy_data of margin pixel (gx, gy) (bmfr.cl:310-484), out of
+// place: the pixel's colour is read from noisy_in and the blended colour
+// goes to the history noisy_out; in-image pixels also write spp,
+// prev_frame_pixel and accept.
+template <typename HistT>
+__device__ __forceinline__ void accumulate_margin_px(
+    const Geometry& g, const AccumArgs& a, int gx, int gy, float2* __restrict__ prev_pix,
+    uint8_t* __restrict__ accept, const float* __restrict__ cur_n, const float* __restrict__ prev_n,
+    const float* __restrict__ cur_p, const float* __restrict__ prev_p, const float* __restrict__ noisy_in,
+    HistT* __restrict__ noisy_out, const HistT* __restrict__ prev_noisy, const uint8_t* __restrict__ prev_spp,
+    uint8_t* __restrict__ cur_spp, void* __restrict__ tmp) {
+    const int2 bo = c_block_offsets[a.frame & 15];
+    const int pwx = gx - kBlockEdge / 2 + bo.x;
+    const int pwy = gy - kBlockEdge / 2 + bo.y;
+    const bool in_image = pwx >= 0 && pwx < g.W && pwy >= 0 && pwy < g.H;
+    const int px = mirror(pwx, g.W), py = mirror(pwy, g.H);
+    const int lp = py * g.W + px;
+    const float3 wp = load3(cur_p, lp);
+    const float3 nrm = load3(cur_n, lp);
+    const float3 cur = load3(noisy_in, lp);
+    const AccumResult r = accumulate_core<HistT>(g, a, px, py, wp, nrm, cur, prev_n, prev_p, prev_noisy, prev_spp);
+    store_tmp_row(g, tmp, a.use_half, gx, gy, wp, nrm, r.color);
+    if (in_image) {   // bmfr.cl:442, 478-484
+        cur_spp[lp] = r.spp;
+        hist_store(noisy_out, lp, r.color);
+        prev_pix[lp] = make_float2(r.ppx, r.ppy);
+        accept[lp] = r.accept;
+    }
+}
+
 // weighted_sum body (bmfr.cl:712-750).
 // Index of the block whose weights pixel (px, py) uses (bmfr.cl:718-722).
 __device__ __forceinline__ int pixel_block(const Geometry& g, int frame, int px, int py) {
@@ -179,6 +209,31 @@ __device__ __forceinline__ float3 accumulate_filtered_px(const Geometry& g, int 
                                   alpha * filt.z + om * prev.z);
     *tm = make_float3(tonemap1(albedo.x, a3.x), tonemap1(albedo.y, a3.y), tonemap1(albedo.z, a3.z));
     return a3;
+}
+
+// weighted_sum followed by accumulate_filtered_data for image pixel (px, py)
+// (bmfr.cl:712-757, 773-856); `filtered` may be null.
+template <typename HistT>
+__device__ __forceinline__ void wsacc_px(const Geometry& g, int frame, float second_alpha, int px, int py,
+                                         const float* __restrict__ weights, const float* __restrict__ mins_maxs,
+                                         const float* __restrict__ cur_n, const float* __restrict__ cur_p,
+                                         float* __restrict__ filtered, const float2* __restrict__ prev_pix,
+                                         const uint8_t* __restrict__ accept, const float* __restrict__ albedo,
+                                         float* __restrict__ tone_mapped, const uint8_t* __restrict__ cur_spp,
+                                         const HistT* __restrict__ acc_prev, HistT* __restrict__ acc_cur) {
+    const int lp = py * g.W + px;
+    const int gi = pixel_block(g, frame, px, py);
+    const float3 f = weighted_sum_px(load3(cur_p, lp), load3(cur_n, lp), weights + (size_t)gi * kFeatures * 3,
+                                     mins_maxs + (size_t)gi * kScaled * 2);
+    if (filtered) store3(filtered, lp, f);
+    float3 tm;
+    const uint8_t acc = frame > 0 ? accept[lp] : 0;
+    const float2 pp = acc ? prev_pix[lp] : make_float2(0.f, 0.f);
+    const uint8_t spp = acc ? cur_spp[lp] : 1;
+    const float3 a3 = accumulate_filtered_px(g, frame, lp, f, pp, acc, spp, second_alpha, acc_prev,
+                                             load3(albedo, lp), &tm);
+    hist_store(acc_cur, lp, a3);
+    store3(tone_mapped, lp, tm);
 }
 
 // taa body (bmfr.cl:873-973).

@@ -31,6 +31,11 @@ __global__ void __launch_bounds__(256) k_accumulate_noisy(
     const uint8_t* __restrict__ prev_spp, uint8_t* __restrict__ cur_spp, void* __restrict__ tmp) {
     const int gx = blockIdx.x * 32 + threadIdx.x;
     const int gy = blockIdx.y * 8 + threadIdx.y;
+    if constexpr (MODE == 0) {
+        accumulate_margin_px<HistT>(g, a, gx, gy, prev_pix, accept, cur_n, prev_n, cur_p, prev_p, noisy_in, noisy_out,
+                                    prev_noisy, prev_spp, cur_spp, tmp);
+        return;
+    }
     const int2 bo = c_block_offsets[a.frame & 15];
     const int pwx = gx - kBlockEdge / 2 + bo.x;
     const int pwy = gy - kBlockEdge / 2 + bo.y;
@@ -106,19 +111,8 @@ __global__ void __launch_bounds__(256) k_weighted_sum_accumulate(
     HistT* __restrict__ acc_cur) {
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
     if (px >= g.W || py >= g.H) return;
-    const int lp = py * g.W + px;
-    const int gi = pixel_block(g, frame, px, py);
-    const float3 f = weighted_sum_px(load3(cur_p, lp), load3(cur_n, lp), weights + (size_t)gi * kFeatures * 3,
-                                     mins_maxs + (size_t)gi * kScaled * 2);
-    if (filtered) store3(filtered, lp, f);
-    float3 tm;
-    const uint8_t acc = frame > 0 ? accept[lp] : 0;
-    const float2 pp = acc ? prev_pix[lp] : make_float2(0.f, 0.f);
-    const uint8_t spp = acc ? cur_spp[lp] : 1;
-    const float3 a3 = accumulate_filtered_px(g, frame, lp, f, pp, acc, spp, second_alpha, acc_prev,
-                                             load3(albedo, lp), &tm);
-    hist_store(acc_cur, lp, a3);
-    store3(tone_mapped, lp, tm);
+    wsacc_px<HistT>(g, frame, second_alpha, px, py, weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept,
+                    albedo, tone_mapped, cur_spp, acc_prev, acc_cur);
 }
 
 constexpr int kTaaRows = 8;

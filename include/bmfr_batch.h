@@ -3,11 +3,14 @@
  * The reference denoises one stream on one in-order queue
  * (opencl/bmfr.cpp:191, 417-485); this layer has no counterpart there.  A
  * batch holds the temporal history of many streams of uneven resolution in
- * HBM and denoises one frame of any subset of them per step: the steps's
- * 32x32 blocks of all those streams form one queue that a single persistent
- * launch walks, and the whole step is one CUDA graph.  Each stream's result
- * is exactly what a plan with the same parameters and the fused pipeline
- * produces for it alone.
+ * HBM and denoises one frame of any subset of them per step, as one CUDA
+ * graph: with params.pipeline = BMFR_PIPELINE_FUSED the step's 32x32 blocks
+ * of all those streams form one queue that a single persistent launch of the
+ * fused block kernel walks; with BMFR_PIPELINE_STAGED persistent launches
+ * walk all streams' margin tiles (accumulation), blocks (fitter) and image
+ * tiles (weighted sum and filtered accumulation).  TAA follows in one more
+ * launch.  Each stream's result is exactly what a plan with the same
+ * parameters (pipeline included) produces for it alone.
  *
  * A server on top admits render streams against a memory budget, queues
  * their frame requests as they arrive and runs steps continuously, so that
@@ -38,15 +41,17 @@ typedef struct bmfr_batch bmfr_batch;
 
 /* Launch parameters of a step, chosen by bmfr_batch_autotune. */
 typedef struct bmfr_batch_tuning {
-    int block_ctas_per_sm;  /* persistent CTAs of the block kernel per SM (0: as many as fit) */
+    int block_ctas_per_sm;  /* persistent CTAs of the block kernel (fused) or fitter (staged) per SM
+                               (0: as many as fit) */
     int taa_tile_w;         /* TAA CTA tile: 30 columns x 16, 32 or 64 rows */
     int taa_tile_h;
-    int staging_depth;      /* 0: blocks from an atomic queue; k > 0: static order with the
-                               inputs of each CTA's next k blocks prefetched into L2 */
+    int staging_depth;      /* fused step: 0 takes blocks from an atomic queue; k > 0 a static
+                               order with the inputs of each CTA's next k blocks prefetched
+                               into L2.  The staged step double-buffers its fitter tiles. */
 } bmfr_batch_tuning;
 
 /* memory_budget_bytes: device bytes the batch's streams may hold (0: no limit).
- * params: shared by every stream; the batch always runs the fused pipeline. */
+ * params: shared by every stream (params.pipeline selects the step's form). */
 int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmfr_batch** batch);
 int bmfr_batch_destroy(bmfr_batch* batch);
 

@@ -1,7 +1,8 @@
 """The many-stream engine (include/bmfr_batch.h): every stream's output in a
-batch step must equal what a plan with the same parameters (fused
-pipeline) produces for that stream alone — bit for bit, since both run the
-same block body — whatever other streams share the step."""
+batch step must equal what a plan with the same parameters (the same
+pipeline, fused or staged) produces for that stream alone — bit for bit,
+since both run the same per-pixel and per-block bodies — whatever other
+streams share the step."""
 import numpy as np
 import pytest
 
@@ -48,11 +49,12 @@ def _device_result(ptr, w, h):
     return device_array(ptr, (h, w, 3), np.float32)
 
 
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_FUSED, B.PIPELINE_STAGED])
 @pytest.mark.parametrize("qr", [B.QR_REFERENCE, B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
-def test_batch_equals_streams_alone(cuda, qr):
+def test_batch_equals_streams_alone(cuda, qr, pipeline):
     import torch
     kw = dict(fp32_qr=qr, half_history=1) if qr != B.QR_REFERENCE else {}
-    params = B.default_params(pipeline=B.PIPELINE_FUSED, **kw)
+    params = B.default_params(pipeline=pipeline, **kw)
     streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
     batch = B.Batch(params)
     slots = [batch.add_stream(s.w, s.h) for s in streams]
@@ -74,9 +76,10 @@ def test_batch_equals_streams_alone(cuda, qr):
     batch.close()
 
 
-def test_batch_autotune_and_budget(cuda):
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_FUSED, B.PIPELINE_STAGED])
+def test_batch_autotune_and_budget(cuda, pipeline):
     import torch
-    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    params = B.default_params(pipeline=pipeline, fp32_qr=1, half_history=1)
     streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES[:3])]
     batch = B.Batch(params)
     slots = [batch.add_stream(s.w, s.h) for s in streams]

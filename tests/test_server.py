@@ -2,7 +2,7 @@
 
 Frames of several streams are submitted while earlier steps run; every
 result must equal what the stream's own plan produces alone (same
-parameters, fused pipeline), streams are admitted against the memory budget,
+parameters and pipeline), streams are admitted against the memory budget,
 and the statistics account for every request.
 """
 import threading
@@ -17,9 +17,10 @@ from test_batch import SIZES, Stream
 pytestmark = pytest.mark.gpu
 
 
-def test_results_alone_and_in_the_mix(cuda):
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_FUSED, B.PIPELINE_STAGED])
+def test_results_alone_and_in_the_mix(cuda, pipeline):
     import torch
-    params = B.default_params(pipeline=B.PIPELINE_FUSED, fp32_qr=1, half_history=1)
+    params = B.default_params(pipeline=pipeline, fp32_qr=1, half_history=1)
     streams = [Stream(k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
     server = B.Server(params)
     ids = [server.open_stream(s.w, s.h) for s in streams]
