@@ -35,6 +35,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from bmfr_b200.replicas import max_over_ranks  # noqa: E402
+
 WIDTH, HEIGHT, FRAMES, SPHERES, SEED = 1280, 720, 60, 12, 20240601
 METRIC = "720p frames/s, full BMFR pipeline (accumulate, fitter, weighted sum, filtered accumulation, TAA)"
 
@@ -265,10 +267,7 @@ def run_batched(args, world, rank, local, dev, barrier, pg):
         e1.record(stream)
         e1.synchronize()
     ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, device=dev)   # the slowest rank
     value = world * n * args.steps / (ms / 1e3)
     batch.close()
 
@@ -760,6 +759,14 @@ def run_precision(args, world, rank, local, dev, barrier, pg):
                 "hh_pixels_over_1e-3": float((eph > 1e-3).double().mean()),
                 "psnr_precision": psnr(out_prec, d["clean"]), "psnr_fp64": psnr(result[c], d["clean"])})
     stream.synchronize()
+    if args.dump_pfm:
+        # The last frame as float images for quality regression: the precision
+        # form, the pipeline with the FP64 fitter, and the noise-free image.
+        out_dir = Path(args.dump_pfm)
+        out_dir.mkdir(parents=True, exist_ok=True)
+        last = F - 1
+        for name, img in (("precision", out_prec), ("fp64", result[last & 1]), ("clean", fr[last]["clean"])):
+            B.write_pfm(out_dir / f"precision_1080p_frame{last}_{name}.pfm", img.cpu().numpy().reshape(H, W, 3))
 
     # Throughput of the precision form and of the plain drop-in at 1080p.
     def time_plan(pl, steps):
@@ -874,6 +881,7 @@ def main():
     ap.add_argument("--frames", type=int, default=FRAMES, help="distinct scene frames held in HBM")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "precision"])
     ap.add_argument("--seconds", type=float, default=10.0, help="served form: length of the arrival trace")
+    ap.add_argument("--dump-pfm", default="", help="precision form: write the last frame's images (PFM) here")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -941,10 +949,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     elapsed_ms = ev0.elapsed_time(ev1)
-    if pg is not None:
-        t = torch.tensor([elapsed_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, device=dev)   # the slowest rank
     value = world * args.steps / (elapsed_ms / 1e3)
     # noise table, block kernel, taa (fused); noise table, accumulate, fitter,
     # weighted_sum, accumulate_filtered, taa (staged)
@@ -998,10 +1003,7 @@ def main():
     e1.record(down_stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, device=dev)   # the slowest rank
     e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": "frames/s",
            "h2d_bytes_per_step": 4 * WIDTH * HEIGHT * 12, "d2h_bytes_per_step": WIDTH * HEIGHT * 12}
 

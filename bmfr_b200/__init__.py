@@ -21,6 +21,7 @@ from ._native import (BatchTuning, ServerConfig, ServerStats, BmfrError, FrameIn
 __all__ = [
     "Plan", "Batch", "Server", "Scene", "BmfrError", "default_params", "block_offsets",
     "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
+    "write_pfm", "read_pfm", "psnr",
     "PIPELINE_FUSED", "PIPELINE_STAGED", "QR_REFERENCE", "QR_CHOLESKY2", "QR_HOUSEHOLDER", "library_path",
 ]
 
@@ -69,6 +70,23 @@ def _ptr(t, name: str, nbytes: int | None = None, optional: bool = False) -> C.c
     if nbytes is not None and t.numel() * t.element_size() < nbytes:
         raise ValueError(f"{name} holds {t.numel() * t.element_size()} bytes, needs {nbytes}")
     return C.c_void_p(t.data_ptr())
+
+
+def _mem_ptr(t, name: str, nbytes: int | None = None) -> C.c_void_p:
+    """Address of host (numpy array, CPU tensor) or device (CUDA tensor) memory."""
+    if isinstance(t, np.ndarray):
+        if not t.flags.c_contiguous:
+            raise ValueError(f"{name} must be contiguous")
+        if nbytes is not None and t.nbytes < nbytes:
+            raise ValueError(f"{name} holds {t.nbytes} bytes, needs {nbytes}")
+        return C.c_void_p(t.ctypes.data)
+    if hasattr(t, "is_cuda") and not t.is_cuda:
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+        if nbytes is not None and t.numel() * t.element_size() < nbytes:
+            raise ValueError(f"{name} holds {t.numel() * t.element_size()} bytes, needs {nbytes}")
+        return C.c_void_p(t.data_ptr())
+    return _ptr(t, name, nbytes)
 
 
 def _f32(values, n: int, name: str):
@@ -388,6 +406,28 @@ class Batch:
         n, sl, iop, keep, mp, op = self._args(slots, io, matrices, offsets)
         check(lib.bmfr_batch_step(self.handle, n, sl, iop, mp, op, _stream_ptr(stream)), "bmfr_batch_step")
 
+    def snapshot_bytes(self, slot: int) -> int:
+        n = C.c_size_t()
+        check(lib.bmfr_batch_snapshot_bytes(self.handle, int(slot), C.byref(n)), "bmfr_batch_snapshot_bytes")
+        return n.value
+
+    def snapshot(self, slot: int, out=None, stream=None):
+        """The stream's history snapshot into `out` (a host numpy uint8 array
+        or a device tensor of snapshot_bytes(slot) bytes; new host array if None)."""
+        n = self.snapshot_bytes(slot)
+        if out is None:
+            out = np.empty(n, dtype=np.uint8)
+        check(lib.bmfr_batch_snapshot(self.handle, int(slot), _mem_ptr(out, "out", n), _stream_ptr(stream)),
+              "bmfr_batch_snapshot")
+        return out
+
+    def restore(self, snapshot, stream=None) -> int:
+        """Adds a stream from a snapshot; returns its slot."""
+        sl = C.c_int()
+        check(lib.bmfr_batch_restore(self.handle, _mem_ptr(snapshot, "snapshot"), _stream_ptr(stream), C.byref(sl)),
+              "bmfr_batch_restore")
+        return sl.value
+
     def result_ptr(self, slot: int) -> int:
         p = C.c_void_p()
         check(lib.bmfr_batch_stream_result(self.handle, int(slot), C.byref(p)), "bmfr_batch_stream_result")
@@ -464,6 +504,19 @@ class Server:
         check(lib.bmfr_server_submit(self.handle, int(sid), C.byref(io) if io is not None else None, mp, op,
                                      C.byref(rid)), "bmfr_server_submit")
         return rid.value
+
+    def snapshot_stream(self, sid: int, out, stream=None):
+        """bmfr_server_snapshot_stream into `out` (host numpy uint8 array or
+        device tensor, at least batch snapshot_bytes long)."""
+        check(lib.bmfr_server_snapshot_stream(self.handle, int(sid), _mem_ptr(out, "out"), _stream_ptr(stream)),
+              "bmfr_server_snapshot_stream")
+        return out
+
+    def restore_stream(self, snapshot, stream=None) -> int:
+        sid = C.c_int()
+        check(lib.bmfr_server_restore_stream(self.handle, _mem_ptr(snapshot, "snapshot"), _stream_ptr(stream),
+                                             C.byref(sid)), "bmfr_server_restore_stream")
+        return sid.value
 
     def poll(self, rid: int):
         done, lat = C.c_int(), C.c_double()
@@ -548,3 +601,38 @@ class Scene:
                                            _ptr(normals, "normals", n), _ptr(positions, "positions", n),
                                            _ptr(noisy, "noisy", n), _ptr(clean, "clean", n, optional=True),
                                            _stream_ptr(stream)), "bmfr_scene_render_device")
+
+
+# -- image output (include/bmfr_image.h) -----------------------------------
+
+def _host_f32(img, name):
+    a = np.ascontiguousarray(img, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def write_pfm(path, image) -> None:
+    """Writes an (H, W, 3) float image (top row first) as a PFM file."""
+    a, p = _host_f32(image, "image")
+    if a.ndim != 3 or a.shape[2] != 3:
+        raise ValueError("image must be (H, W, 3)")
+    check(lib.bmfr_write_pfm(str(path).encode(), a.shape[1], a.shape[0], p), "bmfr_write_pfm")
+
+
+def read_pfm(path) -> np.ndarray:
+    """Reads a colour PFM file as an (H, W, 3) float32 array, top row first."""
+    w, h = C.c_int(), C.c_int()
+    check(lib.bmfr_read_pfm(str(path).encode(), C.byref(w), C.byref(h), None, 0), "bmfr_read_pfm")
+    out = np.empty((h.value, w.value, 3), dtype=np.float32)
+    check(lib.bmfr_read_pfm(str(path).encode(), C.byref(w), C.byref(h), out.ctypes.data_as(C.POINTER(C.c_float)),
+                            out.size), "bmfr_read_pfm")
+    return out
+
+
+def psnr(a, b, peak: float = 1.0) -> float:
+    """PSNR in dB between two float images of the same size."""
+    x, px = _host_f32(a, "a")
+    y, py = _host_f32(b, "b")
+    if x.size != y.size:
+        raise ValueError("images differ in size")
+    return float(lib.bmfr_psnr(px, py, x.size, float(peak)))
+

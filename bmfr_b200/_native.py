@@ -1,4 +1,4 @@
-"""ctypes binding of libbmfr_b200.so (include/bmfr_b200.h, include/bmfr_scene.h).
+"""ctypes binding of libbmfr_b200.so (include/bmfr_b200.h, bmfr_batch.h, bmfr_scene.h, bmfr_image.h).
 
 The library is the product: importing this module loads it and raises if it
 is missing — there is no fallback implementation.
@@ -156,6 +156,11 @@ def _load() -> C.CDLL:
         "bmfr_batch_stream_inputs": (i, [vp, i, C.POINTER(FrameInputs)]),
         "bmfr_batch_step": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, vp]),
         "bmfr_batch_stream_result": (i, [vp, i, C.POINTER(vp)]),
+        "bmfr_batch_snapshot_bytes": (i, [vp, i, C.POINTER(C.c_size_t)]),
+        "bmfr_batch_snapshot": (i, [vp, i, vp, vp]),
+        "bmfr_batch_restore": (i, [vp, vp, vp, C.POINTER(i)]),
+        "bmfr_server_snapshot_stream": (i, [vp, i, vp, vp]),
+        "bmfr_server_restore_stream": (i, [vp, vp, vp, C.POINTER(i)]),
         "bmfr_batch_get_tuning": (i, [vp, C.POINTER(BatchTuning)]),
         "bmfr_batch_set_tuning": (i, [vp, C.POINTER(BatchTuning)]),
         "bmfr_batch_autotune": (i, [vp, i, C.POINTER(i), C.POINTER(FrameIO), fp, fp, i, vp,
@@ -179,6 +184,9 @@ def _load() -> C.CDLL:
         "bmfr_scene_pixel_offset": (i, [C.POINTER(SceneDesc), i, fp]),
         "bmfr_scene_render": (i, [C.POINTER(SceneDesc), i, fp, fp, fp, fp, fp, i]),
         "bmfr_scene_render_device": (i, [C.POINTER(SceneDesc), i, vp, vp, vp, vp, vp, vp]),
+        "bmfr_write_pfm": (i, [C.c_char_p, i, i, fp]),
+        "bmfr_read_pfm": (i, [C.c_char_p, C.POINTER(i), C.POINTER(i), fp, C.c_size_t]),
+        "bmfr_psnr": (C.c_double, [fp, fp, C.c_size_t, f]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

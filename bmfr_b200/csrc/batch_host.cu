@@ -498,6 +498,131 @@ int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io*
     return BMFR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Layout of a stream snapshot: this header, then the histories the next
+// frame reads (those written by the stream's last frame): accumulated noisy
+// colour, accumulated filtered colour, TAA result, spp, and with own input
+// slots the previous normals and positions.
+struct SnapshotHeader {
+    char magic[8];   // "BMFRSNP1"
+    int32_t width, height, frame, own_inputs;
+    int32_t half_history, use_half, pipeline, fp32_qr;
+    uint64_t payload_bytes;
+};
+
+struct HistoryPart {
+    void* ptr;
+    size_t bytes;
+};
+
+// The slot's history buffers that frame `frame` reads, in snapshot order.
+std::vector<HistoryPart> history_parts(const bmfr_batch* b, const StreamSlot& s, int frame) {
+    const size_t px = (size_t)s.width * s.height;
+    const size_t hist = px * 3 * (b->p.half_history ? 2 : 4);
+    const int prv = (frame & 1) ^ 1;
+    std::vector<HistoryPart> parts = {{s.noisy_acc[prv], hist}, {s.acc_filt[prv], hist}, {s.result[prv], hist},
+                                      {s.spp[prv], px}};
+    if (s.own_inputs) {
+        parts.push_back({s.normals[prv], px * 12});
+        parts.push_back({s.positions[prv], px * 12});
+    }
+    return parts;
+}
+
+size_t payload_bytes(const std::vector<HistoryPart>& parts) {
+    size_t n = 0;
+    for (const HistoryPart& h : parts) n += h.bytes;
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bmfr_batch_snapshot_bytes(const bmfr_batch* b, int slot, size_t* bytes) {
+    if (!b || !bytes) return fail(BMFR_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (int st = check_slot(b, slot)) return st;
+    const StreamSlot& s = b->slots[slot];
+    *bytes = sizeof(SnapshotHeader) + payload_bytes(history_parts(b, s, s.frame));
+    return BMFR_OK;
+}
+
+int bmfr_batch_snapshot(bmfr_batch* b, int slot, void* dst, void* stream) {
+    if (int st = check_batch(b)) return st;
+    if (!dst) return fail(BMFR_E_INVALID, "snapshot: NULL destination");
+    cudaStream_t cs = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (int st = check_slot(b, slot)) return st;
+    const StreamSlot& s = b->slots[slot];
+    const std::vector<HistoryPart> parts = history_parts(b, s, s.frame);
+    SnapshotHeader h{};
+    std::memcpy(h.magic, "BMFRSNP1", 8);
+    h.width = s.width;
+    h.height = s.height;
+    h.frame = s.frame;
+    h.own_inputs = s.own_inputs ? 1 : 0;
+    h.half_history = b->p.half_history ? 1 : 0;
+    h.use_half = b->p.use_half_precision_in_tmp_data ? 1 : 0;
+    h.pipeline = b->p.pipeline;
+    h.fp32_qr = b->p.fp32_qr;
+    h.payload_bytes = payload_bytes(parts);
+    cudaError_t e = cudaSuccess;
+    if (b->last >= 0) e = cudaStreamWaitEvent(cs, b->done[b->last], 0);   // after the stream's last step
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, &h, sizeof h, cudaMemcpyDefault, cs);
+    char* out = static_cast<char*>(dst) + sizeof h;
+    for (const HistoryPart& part : parts) {
+        if (e != cudaSuccess) break;
+        e = cudaMemcpyAsync(out, part.ptr, part.bytes, cudaMemcpyDefault, cs);
+        out += part.bytes;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "snapshot copies");
+}
+
+int bmfr_batch_restore(bmfr_batch* b, const void* src, void* stream, int* slot) {
+    if (int st = check_batch(b)) return st;
+    if (!src || !slot) return fail(BMFR_E_INVALID, "restore: NULL argument");
+    cudaStream_t cs = (cudaStream_t)stream;
+    SnapshotHeader h{};
+    cudaError_t e = cudaMemcpy(&h, src, sizeof h, cudaMemcpyDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "restore: reading the header");
+    if (std::memcmp(h.magic, "BMFRSNP1", 8) != 0) return fail(BMFR_E_INVALID, "restore: not a stream snapshot");
+    if (h.half_history != (b->p.half_history ? 1 : 0) || h.use_half != (b->p.use_half_precision_in_tmp_data ? 1 : 0))
+        return fail(BMFR_E_INVALID, "restore: the snapshot's history format differs from the batch's");
+    if (h.frame < 0) return fail(BMFR_E_INVALID, "restore: bad frame counter");
+    int k = -1;
+    if (int st = bmfr_batch_add_stream(b, h.width, h.height, h.own_inputs, &k)) return st;
+    std::vector<HistoryPart> parts;
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        StreamSlot& s = b->slots[k];
+        parts = history_parts(b, s, h.frame);
+        if (payload_bytes(parts) != h.payload_bytes) {
+            free_slot(b, s);
+            return fail(BMFR_E_INVALID, "restore: snapshot size does not match the stream");
+        }
+        s.frame = h.frame;
+    }
+    e = cudaStreamWaitEvent(cs, b->mem_ready, 0);   // the slot's memory is allocated and zeroed
+    const char* in = static_cast<const char*>(src) + sizeof h;
+    for (const HistoryPart& part : parts) {
+        if (e != cudaSuccess) break;
+        e = cudaMemcpyAsync(part.ptr, in, part.bytes, cudaMemcpyDefault, cs);
+        in += part.bytes;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) {
+        bmfr_batch_remove_stream(b, k);
+        return cuda_fail(e, "restore copies");
+    }
+    *slot = k;
+    return BMFR_OK;
+}
+
 int bmfr_batch_stream_result(const bmfr_batch* b, int slot, const float** result) {
     if (!b || !result) return fail(BMFR_E_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lk(b->mu);

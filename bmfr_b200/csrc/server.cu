@@ -285,6 +285,30 @@ int bmfr_server_close_stream(bmfr_server* s, int id) {
     return bmfr_batch_remove_stream(s->batch, id);
 }
 
+int bmfr_server_snapshot_stream(bmfr_server* s, int id, void* dst, void* stream) {
+    if (!s) return fail(BMFR_E_INVALID, "server is NULL");
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (!s->open.count(id)) return fail(BMFR_E_NOT_FOUND, "no open stream " + std::to_string(id));
+        // Its submitted frames finish first.
+        s->cv_done.wait(lk, [&] { return s->open[id] == 0 || !s->thread_error.empty(); });
+        if (!s->thread_error.empty()) return fail(BMFR_E_STATE, "server step failed: " + s->thread_error);
+    }
+    return bmfr_batch_snapshot(s->batch, id, dst, stream);
+}
+
+int bmfr_server_restore_stream(bmfr_server* s, const void* src, void* stream, int* id) {
+    if (!s || !id) return fail(BMFR_E_INVALID, "NULL argument");
+    const int st = bmfr_batch_restore(s->batch, src, stream, id);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (st == BMFR_E_BUDGET) s->rejected += 1;
+    if (st != BMFR_OK) return st;
+    s->admitted += 1;
+    s->pending[*id];
+    s->open[*id] = 0;
+    return BMFR_OK;
+}
+
 int bmfr_server_stream_inputs(bmfr_server* s, int id, bmfr_frame_inputs* in) {
     if (!s) return fail(BMFR_E_INVALID, "server is NULL");
     return bmfr_batch_stream_inputs(s->batch, id, in);

@@ -87,6 +87,20 @@ int bmfr_batch_stream_inputs(bmfr_batch* batch, int slot, bmfr_frame_inputs* inp
 int bmfr_batch_step(bmfr_batch* batch, int n, const int* slots, const bmfr_frame_io* io,
                     const float* matrices, const float* offsets, void* stream);
 
+/* Per-stream history snapshot, for moving a stream to another batch or GPU
+ * between frames (no counterpart in the reference).  A snapshot holds the
+ * stream's size and frame counter and the histories its next frame reads
+ * (accumulated noisy and filtered colour, TAA result, spp; with input slots
+ * the previous normals and positions).  bmfr_batch_snapshot copies it to
+ * `dst` (host or device memory, bmfr_batch_snapshot_bytes long) after the
+ * stream's last step and returns when the copy is done.  bmfr_batch_restore
+ * adds a stream from a snapshot taken with the same history format
+ * (half_history, tmp type) and returns its slot; its next frame continues
+ * the sequence exactly as the original stream's would. */
+int bmfr_batch_snapshot_bytes(const bmfr_batch* batch, int slot, size_t* bytes);
+int bmfr_batch_snapshot(bmfr_batch* batch, int slot, void* dst, void* stream);
+int bmfr_batch_restore(bmfr_batch* batch, const void* src, void* stream, int* slot);
+
 /* Float output of the stream's last denoised frame (device, W*H*3). */
 int bmfr_batch_stream_result(const bmfr_batch* batch, int slot, const float** result);
 
@@ -137,6 +151,11 @@ int bmfr_server_open_stream(bmfr_server* server, int width, int height, int* str
 /* Waits for the stream's queued frames, then frees its memory. */
 int bmfr_server_close_stream(bmfr_server* server, int stream_id);
 int bmfr_server_stream_inputs(bmfr_server* server, int stream_id, bmfr_frame_inputs* inputs);
+/* bmfr_batch_snapshot of an open stream once its submitted frames are done
+ * (the stream stays open), and bmfr_batch_restore as an admitted stream:
+ * moving a render stream between servers or GPUs between two frames. */
+int bmfr_server_snapshot_stream(bmfr_server* server, int stream_id, void* dst, void* stream);
+int bmfr_server_restore_stream(bmfr_server* server, const void* src, void* stream, int* stream_id);
 
 /* Queues the stream's next frame.  io: the frame's device buffers (they and
  * the previous G-buffer pointers must stay valid until the request

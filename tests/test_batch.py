@@ -107,3 +107,36 @@ def test_batch_autotune_and_budget(cuda, pipeline):
     assert small.bytes_in_use == need
     small.close()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("to_device", [False, True])
+def test_snapshot_and_restore(cuda, to_device):
+    """A stream snapshotted between frames and restored into another batch
+    continues exactly as the original: the next frames are bit-identical."""
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_STAGED, fp32_qr=1, half_history=1)
+    st = Stream(3, 160, 96, params, cuda)
+    a = B.Batch(params)
+    sa = a.add_stream(st.w, st.h)
+
+    def step(batch, slot, f):
+        batch.step([slot], st.sc.prev_camera(f), st.sc.pixel_offset(f), io=[st.io(f)])
+        return _device_result(batch.result_ptr(slot), st.w, st.h)
+
+    for f in range(4):
+        step(a, sa, f)
+    n = a.snapshot_bytes(sa)
+    snap = a.snapshot(sa, out=torch.empty(n, dtype=torch.uint8, device=cuda) if to_device else None)
+    want = [step(a, sa, f) for f in range(4, 7)]
+    b = B.Batch(params)
+    b.add_stream(64, 64)            # another stream first, so the slot differs
+    sb = b.restore(snap)
+    assert b.frame(sb) == 4
+    for k, f in enumerate(range(4, 7)):
+        np.testing.assert_array_equal(step(b, sb, f), want[k], err_msg=f"frame {f}")
+    other = B.Batch(B.default_params(pipeline=B.PIPELINE_STAGED))   # float histories: another format
+    with pytest.raises(B.BmfrError):
+        other.restore(snap)
+    for x in (a, b, other):
+        x.close()
+    torch.cuda.synchronize()

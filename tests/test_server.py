@@ -78,3 +78,35 @@ def test_admission_against_the_budget(cuda):
     with pytest.raises(B.BmfrError):
         server.submit(999, np.eye(4), [0.5, 0.5])   # never opened
     server.close()
+
+
+def test_stream_moves_between_servers(cuda):
+    """A stream snapshotted in one server and restored in another carries on
+    with identical frames (serving migration between two frames)."""
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_STAGED, fp32_qr=1, half_history=1)
+    st = Stream(2, 128, 128, params, cuda)
+    one, two = B.Server(params), B.Server(params)
+    sid = one.open_stream(st.w, st.h)
+
+    def submit(server, s, f):
+        out = torch.empty(st.w * st.h * 3, dtype=torch.float32, device=cuda)
+        io = st.io(f)
+        io.result = out.data_ptr()
+        server.submit(s, st.sc.prev_camera(f), st.sc.pixel_offset(f), io=io)
+        return out
+
+    for f in range(3):
+        submit(one, sid, f)
+    snap = np.empty(B.Batch.stream_bytes(params, st.w, st.h), dtype=np.uint8)   # at least the snapshot's size
+    one.snapshot_stream(sid, snap)
+    want = [submit(one, sid, f) for f in range(3, 6)]
+    one.drain()
+    moved = two.restore_stream(snap)
+    got = [submit(two, moved, f) for f in range(3, 6)]
+    two.drain()
+    torch.cuda.synchronize()
+    for k in range(3):
+        np.testing.assert_array_equal(got[k].cpu().numpy(), want[k].cpu().numpy(), err_msg=f"frame {3 + k}")
+    one.close()
+    two.close()
