@@ -168,12 +168,12 @@ __device__ __forceinline__ float3 weighted_sum_px(float3 wp, float3 n, const flo
 // colour and writes the tone-mapped one through `tm`.
 // Tone map: clamp(powr(max(0, albedo * acc), 0.454545), 0, 1) (bmfr.cl:853-854).
 // powr is evaluated as exp2(0.454545 * log2(x)) on the special function
-// unit (__log2f, __exp2f): relative error below 1e-6 for x above 1e-3 and a
+// unit (__log2f, exp2f): relative error below 1e-6 for x above 1e-3 and a
 // negligible absolute error below that (the OpenCL powr it stands for may
 // be 16 ulp off); several times cheaper than powf.
 __device__ __forceinline__ float tonemap1(float albedo, float acc) {
     const float x = fmax_cl(0.0f, albedo * acc);
-    const float t = x > 0.0f ? __exp2f(0.454545f * __log2f(x)) : 0.0f;
+    const float t = x > 0.0f ? exp2f(0.454545f * __log2f(x)) : 0.0f;
     return fmin_cl(fmax_cl(t, 0.0f), 1.0f);
 }
 
