@@ -96,6 +96,27 @@ def build_oracle(verbose: bool = False) -> Path:
     return oracle / "libbmfr_oracle.so"
 
 
+REFERENCE_CL = Path("/root/reference/opencl/bmfr.cl")
+
+
+def build_reference(verbose: bool = False) -> Path | None:
+    """Compiles the reference's own kernels for the CPU (test
+    infrastructure: oracle/ref_cl -> oracle/_ref/libbmfr_ref.so) when the
+    reference source is present; otherwise keeps a library built earlier."""
+    oracle = ROOT / "oracle"
+    if not REFERENCE_CL.exists():
+        lib = oracle / "_ref" / "libbmfr_ref.so"
+        return lib if lib.exists() else None
+    r = subprocess.run(["make", "-C", str(oracle), "ref", f"REF_SRC={REFERENCE_CL}", f"PYTHON={sys.executable}"],
+                       capture_output=True, text=True)
+    if verbose:
+        print(r.stdout, r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError(f"building the reference kernels failed:\n{r.stdout}\n{r.stderr}")
+    return oracle / "_ref" / "libbmfr_ref.so"
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
     print(build_oracle(verbose="-v" in sys.argv))
+    print(build_reference(verbose="-v" in sys.argv))

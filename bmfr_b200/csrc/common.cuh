@@ -68,8 +68,12 @@ struct NoiseConst {
     float hi, lo;
 };
 
-__device__ __forceinline__ float fmin_cl(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float fmax_cl(float a, float b) { return b > a ? b : a; }
+// OpenCL's fmin/fmax (and max(x, y) for the operands the kernels give it):
+// y if y < x (x < y), else x; the other operand when x is NaN.  A NaN
+// reaches them in taa when every bilinear weight of the history is zero
+// (bmfr.cl:939: 0/0), and the clamp then returns the bound.
+__device__ __forceinline__ float fmin_cl(float x, float y) { return (y < x || x != x) ? y : x; }
+__device__ __forceinline__ float fmax_cl(float x, float y) { return (x < y || x != x) ? y : x; }
 
 // mirror (bmfr.cl:209-216): valid for indices at most one size out of range.
 __device__ __forceinline__ int mirror(int i, int n) {

@@ -334,9 +334,9 @@ __device__ __forceinline__ float3 taa_core(const Geometry& g, int frame, float t
 // keeps a three-row window of horizontal minima and maxima, so a pixel's
 // nine neighbours cost about one load and one YCoCg conversion.  Neighbours
 // outside the image or NaN enter as +-inf, which the reference's fmin/fmax
-// ignore in the same way (bmfr.cl:884-902; fmin_cl keeps its first operand
-// on a NaN), so the bounds equal the reference's up to the sign of a zero
-// bound.
+// ignore in the same way (bmfr.cl:884-902; fmin/fmax return the other
+// operand of a NaN), so the bounds equal the reference's up to the sign of a
+// zero bound.
 template <int R, typename HistT>
 __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float taa_alpha, int x0, int y0,
                                           const float2* __restrict__ prev_pix, const float* __restrict__ new_frame,

@@ -2,9 +2,9 @@
 // reference's OpenCL kernels (opencl/bmfr.cl), the parity checker of the CUDA
 // pipeline and the timed CPU baseline.  Nothing in the product links this.
 //
-// PARITY UNPINNED: the reference has no tests, golden vectors or fixtures,
-// and its OpenCL kernels cannot run on either machine of this build, so the
-// restatement is pinned only by hand-derived known-answer tests.
+// PINNED to the reference itself: the reference's own kernels, compiled for
+// the CPU by oracle/ref_cl, give bit-identical outputs on the same inputs
+// (tests/test_reference_pin.py, fixtures in tests/golden/).
 //
 // Arithmetic rules (compiled with -ffp-contract=off, no fast-math):
 //  * every float expression keeps the reference's evaluation order, one
@@ -15,7 +15,9 @@
 //  * convert_int2_rtn is floor; NaN and values beyond +-2^30 map to -2^30 /
 //    +2^30 so that they land outside every image (OpenCL leaves the
 //    conversion of out-of-range values undefined);
-//  * fmin/fmax are (b < a ? b : a) / (b > a ? b : a); no NaN reaches them;
+//  * fmin/fmax are (y < x ? y : x) / (x < y ? y : x), returning the other
+//    operand when x is NaN (the specification's NaN rule; max(0, v) of the
+//    tone map gives the same values);
 //  * the fitter's work-group reductions are evaluated over the same tree as
 //    parallel_reduction_sum/min/max (bmfr.cl:25-87).
 #include "bmfr_oracle.h"
@@ -46,8 +48,10 @@ const int kBlockOffsets[16][2] = {
 
 inline float half_round(float v) { return (float)(_Float16)v; }
 
-inline float fmin_cl(float a, float b) { return b < a ? b : a; }
-inline float fmax_cl(float a, float b) { return b > a ? b : a; }
+// OpenCL fmin/fmax: y if y < x (x < y), else x; the other operand when x is
+// NaN (a NaN reaches the clamp of taa when all history weights are zero).
+inline float fmin_cl(float x, float y) { return (y < x || x != x) ? y : x; }
+inline float fmax_cl(float x, float y) { return (x < y || x != x) ? y : x; }
 
 // convert_int_rtn with defined results outside the int range.
 inline int floor_to_int(float v) {

@@ -4,10 +4,11 @@
  * used as the parity checker of the CUDA pipeline and as the timed CPU
  * baseline.  Nothing in the product links or calls this library.
  *
- * PARITY UNPINNED: the reference ships no tests, golden vectors or fixtures
- * (its dataset and camera_matrices.h are absent), and its OpenCL kernels
- * cannot run on either machine of this build (no OpenCL platform), so this
- * restatement is checked only by hand-derived known-answer tests.
+ * PINNED to the reference itself: the reference's own kernels (opencl/bmfr.cl)
+ * are compiled for the CPU by oracle/ref_cl (g++ through an OpenCL C
+ * compatibility header, a fiber per work-item) and every output of this
+ * restatement equals theirs bit for bit, intermediates included
+ * (tests/test_reference_pin.py; fixtures in tests/golden/).
  *
  * All buffers are HOST memory with the reference's layouts.
  */

@@ -4,8 +4,9 @@
 Only tests, the smoke check and the CPU-baseline leg of bench.py use this
 module, as the checker; the product never imports it.
 
-PARITY UNPINNED: the reference ships no golden vectors and cannot run here,
-so this oracle is checked only against hand-derived known-answer tests.
+Pinned to the reference itself: the reference's own kernels, compiled for
+the CPU by oracle/ref_cl (oracle/ref.py), give bit-identical outputs on the
+same inputs (tests/test_reference_pin.py, fixtures in tests/golden/).
 """
 from __future__ import annotations
 

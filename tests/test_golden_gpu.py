@@ -1,0 +1,130 @@
+"""The CUDA path against the reference's own outputs.
+
+tests/golden/ref_*.npz hold outputs of the reference's OpenCL kernels
+(opencl/bmfr.cl compiled for the CPU, tests/golden/make_golden.py) with the
+inputs that produced them: a three-frame run of the procedural scene, and one
+frame of edge inputs for every stage (NaN, infinities, values beyond
+binary16, spp 0 and 255, degenerate blocks, reprojections on and beyond the
+image edges).  The plan pipeline (staged and fused) and the five drop-in
+entry points are run on the stored inputs.  Integer outputs, tmp_data and the
+accumulations must be bit-identical (NaN equal to NaN); the fitted weights
+bit-identical in more than 99 % of values (the noise term, see the fitter);
+tone mapping (powr on the special function unit) and TAA within 1e-5.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import bmfr_b200 as B
+
+from test_parity_pipeline import device_array
+from test_parity_stages import assert_close
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def same(a, b, what):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape, what
+    eq = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else a == b
+    assert eq.all(), f"{what}: {int((~eq).sum())} of {eq.size} values differ"
+
+
+def weights_match(got, want, what):
+    got, want = np.asarray(got), np.asarray(want)
+    assert (np.isnan(got) == np.isnan(want)).all(), f"{what}: NaN pattern differs"
+    fin = ~np.isnan(want)
+    exact = (got[fin] == want[fin]).mean()
+    assert exact > 0.99, f"{what}: bit-identical fraction {exact:.4f}"
+
+
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
+def test_plan_pipeline_matches_reference_fixture(cuda, pipeline):
+    g = np.load(GOLDEN / "ref_pipeline.npz")
+    frames = sum(1 for k in g.files if k.endswith("_result"))
+    H, W = g["in0_albedo"].shape[:2]
+    lim = g["limits"]
+    plan = B.Plan(W, H, pipeline=pipeline, position_limit_squared=float(lim[0]),
+                  normal_limit_squared=float(lim[1]))
+    for f in range(frames):
+        plan.upload_frame(g[f"in{f}_albedo"], g[f"in{f}_normals"], g[f"in{f}_positions"], g[f"in{f}_noisy"])
+        plan.denoise_frame(g[f"in{f}_matrix"], g[f"in{f}_offset"])
+        got = plan.download_result()
+        bufs = plan.buffers()
+        same(device_array(bufs.accept, (H, W), np.uint8), g[f"out{f}_accept"], f"accept {f}")
+        same(device_array(bufs.spp, (H, W), np.uint8), g[f"out{f}_spp"], f"spp {f}")
+        same(device_array(bufs.prev_frame_pixel, (H, W, 2), np.float32), g[f"out{f}_prev_pix"], f"prev pix {f}")
+        same(device_array(bufs.mins_maxs, g[f"out{f}_mins_maxs"].shape, np.float32), g[f"out{f}_mins_maxs"],
+             f"mins_maxs {f}")
+        weights_match(device_array(bufs.weights, g[f"out{f}_weights"].shape, np.float32), g[f"out{f}_weights"],
+                      f"weights {f}")
+        same(device_array(bufs.accumulated_noisy, (H, W, 3), np.float32), g[f"out{f}_noisy_acc"],
+             f"accumulated noisy {f}")
+        assert_close(device_array(bufs.tone_mapped, (H, W, 3), np.float32), g[f"out{f}_tone_mapped"],
+                     f"tone mapped {f}", rtol=1e-5)
+        assert_close(got, g[f"out{f}_result"], f"result {f}", rtol=1e-4)
+    plan.close()
+
+
+def test_dropin_stages_match_reference_edge_fixture(cuda):
+    import torch
+    g = np.load(GOLDEN / "ref_stages.npz")
+    H, W = g["in_albedo"].shape[:2]
+    px = W * H
+    f = int(g["in_frame"][0])
+    plan = B.Plan(W, H, position_limit_squared=float(g["in_limits"][0]),
+                  normal_limit_squared=float(g["in_limits"][1]))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+    n = lambda x: x.detach().cpu().numpy()
+    blocks = g["out_fit_weights"].size // 30
+
+    # accumulate_noisy_data
+    g_pp = torch.zeros(px * 2, dtype=torch.float32, device=cuda)
+    g_acc = torch.zeros(px, dtype=torch.uint8, device=cuda)
+    g_spp = torch.zeros(px, dtype=torch.uint8, device=cuda)
+    g_tmp = torch.zeros(blocks * 13 * 1024, dtype=torch.float16, device=cuda)
+    g_noisy = t(g["in_cur_noisy"])
+    B.accumulate_noisy_data(plan, g_pp, g_acc, t(g["in_cur_normals"]), t(g["in_prev_normals"]),
+                            t(g["in_cur_positions"]), t(g["in_prev_positions"]), g_noisy, t(g["in_prev_noisy"]),
+                            t(g["in_prev_spp"]), g_spp, g_tmp, g["in_matrix"], g["in_offset"], f)
+    torch.cuda.synchronize()
+    same(n(g_pp).reshape(H, W, 2), g["out_acc_prev_pix"], "prev_frame_pixel")
+    same(n(g_acc).reshape(H, W), g["out_acc_accept"], "accept")
+    same(n(g_spp).reshape(H, W), g["out_acc_spp"], "spp")
+    same(n(g_tmp).view(np.uint16), g["out_acc_tmp"].view(np.uint16), "tmp_data")
+    same(n(g_noisy).reshape(H, W, 3), g["out_acc_noisy"], "accumulated noisy")
+
+    # fitter (constant, all-zero and +-65504 blocks among the scene's)
+    g_w = torch.zeros(blocks * 30, dtype=torch.float32, device=cuda)
+    g_mm = torch.zeros(blocks * 12, dtype=torch.float32, device=cuda)
+    B.fitter(plan, g_w, g_mm, t(g["in_fit_tmp"]), f)
+    torch.cuda.synchronize()
+    same(n(g_mm), g["out_fit_mins_maxs"], "mins_maxs")
+    weights_match(n(g_w), g["out_fit_weights"], "weights")
+
+    # weighted_sum on the reference's weights (NaN blocks included)
+    g_out = torch.zeros(px * 3, dtype=torch.float32, device=cuda)
+    B.weighted_sum(plan, t(g["out_fit_weights"]), t(g["out_fit_mins_maxs"]), g_out, t(g["in_cur_normals"]),
+                   t(g["in_cur_positions"]), None, f)
+    torch.cuda.synchronize()
+    same(n(g_out).reshape(H, W, 3), g["out_ws_filtered"], "weighted sum")
+
+    # accumulate_filtered_data (spp 0, taps on every edge)
+    g_tm = torch.zeros(px * 3, dtype=torch.float32, device=cuda)
+    g_acc_cur = torch.zeros(px * 3, dtype=torch.float32, device=cuda)
+    B.accumulate_filtered_data(plan, t(g["out_ws_filtered"]), t(g["in_prev_pix"]), t(g["in_accept"]),
+                               t(g["in_albedo"]), g_tm, t(g["in_cur_spp"]), t(g["in_acc_prev"]), g_acc_cur, f)
+    torch.cuda.synchronize()
+    same(n(g_acc_cur).reshape(H, W, 3), g["out_af_accumulated"], "accumulated filtered")
+    assert_close(n(g_tm).reshape(H, W, 3), g["out_af_tone_mapped"], "tone mapped", rtol=1e-5)
+
+    # taa (history positions NaN, infinite, at -1 and on the last row)
+    g_res = torch.zeros(px * 3, dtype=torch.float32, device=cuda)
+    B.taa(plan, t(g["in_taa_prev_pix"]), t(g["out_af_tone_mapped"]), g_res, t(g["in_taa_prev"]), f)
+    torch.cuda.synchronize()
+    assert_close(n(g_res).reshape(H, W, 3), g["out_taa_result"], "taa", rtol=1e-5)
+    plan.close()
+
