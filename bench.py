@@ -13,7 +13,8 @@ Our arm prints one JSON line with
              four input uploads and the result download inside the timed region,
   stages     ms per stage (the reference's per-kernel profile, bmfr.cpp:488-517),
   roofline   the dominant kernel's achieved HBM bandwidth against the measured
-             copy bandwidth,
+             copy bandwidth, and (`issue`) its warp-instruction rate against
+             the SMs' issue rate, the bound of an issue-bound kernel,
   cpu_baseline  the reference's own OpenCL kernels compiled for the CPU
              (oracle/_ref) on a bounded sample of frames on this host's cores,
              with the oracle port's figure beside it.
@@ -82,6 +83,12 @@ def stage_bytes(w, h):
 # the kernel (profiles/*_720p.md: `bench.py --form probe --frames 3 --qr 0`).
 NCU_TRAFFIC_720P = {"fitter": 26.31e6, "accumulate_noisy_data": 66.8e6, "taa": 26.0e6,
                     "weighted_sum+accumulate_filtered_data": 48.7e6}
+# Warp instructions per launch at 1280x720 (smsp__inst_executed.sum of the
+# same captures): the numerator of the issue-rate roofline of a kernel that
+# is bound by instruction issue rather than by HBM.
+NCU_WARP_INST_720P = {"fitter": 57.9e6, "accumulate_noisy_data": 17.8e6, "taa": 11.0e6,
+                      "weighted_sum+accumulate_filtered_data": 12.4e6}
+SMS, SCHEDULERS_PER_SM = 148, 4
 
 
 def frame_order(i, n):
@@ -1058,6 +1065,15 @@ def main():
     if dominant == "fitter":
         roofline["note"] = ("the fitter is bound by instruction issue (ncu: 58 % issue active, 7.35 k instructions "
                             "per thread per block), not by HBM or tensor cores; stages_gbs shows the HBM-bound stages")
+    clk = clocks.summary()
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    issue_peak = SMS * SCHEDULERS_PER_SM * sm_mhz * 1e6 / 1e9          # G warp-instructions/s
+    if dominant in NCU_WARP_INST_720P:
+        got = NCU_WARP_INST_720P[dominant] / (stages[dominant] * 1e-3) / 1e9
+        roofline["issue"] = {"achieved": got, "peak": issue_peak, "unit": "G warp-instructions/s",
+                             "frac": got / issue_peak, "instructions_per_launch": NCU_WARP_INST_720P[dominant],
+                             "peak_source": f"{SMS} SMs x {SCHEDULERS_PER_SM} schedulers x 1 instruction/cycle at "
+                                            f"the sampled SM clock ({sm_mhz:.0f} MHz)"}
     stage_gbs = {k: sb[k] / (v * 1e-3) / 1e9 for k, v in stages.items() if v > 0}
     dropin = dropin_stage_ms(B, torch, dev, stream, plan.params, devf, mats, off, min(args.steps, 30))
 
@@ -1110,7 +1126,7 @@ def main():
             "dropin_stages_ms": dropin,
             "dropin_stages_gbs": {k: sb[k] / (v * 1e-3) / 1e9 for k, v in dropin.items() if v > 0},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks.summary(), "gpu_launches": launches_per_frame * args.steps,
+            "clocks": clk, "gpu_launches": launches_per_frame * args.steps,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
