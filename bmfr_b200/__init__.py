@@ -205,6 +205,17 @@ class Plan:
     def enable_profiling(self, enable: bool = True) -> None:
         check(lib.bmfr_plan_enable_profiling(self.handle, int(enable)), "bmfr_plan_enable_profiling")
 
+    def check_device(self, stream=None) -> None:
+        """Waits for `stream`; raises BmfrError (BMFR_E_TIMEOUT) if a kernel
+        of this plan gave up a bounded wait, and clears that status."""
+        check(lib.bmfr_plan_check_device(self.handle, _stream_ptr(stream)), "bmfr_plan_check_device")
+
+    def probe_bounded_wait(self, limit_us: int, stream=None) -> None:
+        """Enqueues a wait that runs out after `limit_us` (the failure path
+        of the bounded waits, without a fault); check_device then raises."""
+        check(lib.bmfr_plan_probe_bounded_wait(self.handle, int(limit_us), _stream_ptr(stream)),
+              "bmfr_plan_probe_bounded_wait")
+
     STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data", None, "taa")
     FUSED_STAGES = ("noise_table", "block_kernel", None, None, "taa")
 

@@ -143,6 +143,7 @@ def _load() -> C.CDLL:
         "bmfr_plan_buffers_get": (i, [vp, C.POINTER(PlanBuffers)]),
         "bmfr_plan_enable_profiling": (i, [vp, i]),
         "bmfr_plan_check_device": (i, [vp, vp]),
+        "bmfr_plan_probe_bounded_wait": (i, [vp, C.c_uint, vp]),
         "bmfr_plan_stage_times": (i, [vp, fp]),
         "bmfr_batch_create": (i, [C.POINTER(Params), C.c_size_t, C.POINTER(vp)]),
         "bmfr_batch_destroy": (i, [vp]),

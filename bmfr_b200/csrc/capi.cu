@@ -596,6 +596,14 @@ int bmfr_plan_check_device(const bmfr_plan* plan, void* stream) {
     return BMFR_OK;
 }
 
+int bmfr_plan_probe_bounded_wait(bmfr_plan* plan, unsigned int limit_us, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (limit_us < 1 || limit_us > 1000000) return fail(BMFR_E_INVALID, "limit_us must be within [1, 1000000]");
+    const cudaError_t e = bmfr::launch_bounded_wait_probe(plan->dev_status, 1000ull * limit_us,
+                                                          (cudaStream_t)stream);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "probe_bounded_wait");
+}
+
 int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable) {
     if (int st = check_plan(plan)) return st;
     if (enable && !plan->events[0]) {

@@ -147,6 +147,23 @@ cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// A barrier that no copy or thread ever completes: thread 0's bounded wait
+// runs out after limit_ns and records the timeout as the fitter does.
+__global__ void __launch_bounds__(32) k_bounded_wait_probe(int* __restrict__ status, unsigned long long limit_ns) {
+    __shared__ alignas(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, limit_ns)) atomicExch(status, kDevTimeout);
+}
+
+cudaError_t launch_bounded_wait_probe(int* status, unsigned long long limit_ns, cudaStream_t s) {
+    k_bounded_wait_probe<<<1, 32, 0, s>>>(status, limit_ns);
+    return cudaGetLastError();
+}
+
 // cuTensorMapEncodeTiled from the driver, looked up once.
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static std::once_flag once;

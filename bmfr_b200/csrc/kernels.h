@@ -27,6 +27,10 @@ cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const voi
                           int qr, float* weights, float* mins_maxs, const float* noise_table, int* status,
                           cudaStream_t s);
 cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s);
+// One CTA waits, with the fitter's bounded wait limited to limit_ns, on a
+// barrier that nothing completes, and records kDevTimeout in `status` when
+// the limit runs out: the failure path of the bounded waits, without a fault.
+cudaError_t launch_bounded_wait_probe(int* status, unsigned long long limit_ns, cudaStream_t s);
 // The fitter with its scratch in a static device array (no allocation).
 cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
                                  int qr, float* weights, float* mins_maxs, cudaStream_t s);

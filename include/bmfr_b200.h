@@ -298,6 +298,14 @@ int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);
  * without end. */
 int bmfr_plan_check_device(const bmfr_plan* plan, void* stream);
 
+/* Diagnostics of the failure path above: enqueues on `stream` one CTA that
+ * waits, with the fitter's bounded wait limited to `limit_us`
+ * (1..1,000,000), on a barrier that nothing completes.  The wait runs out,
+ * the timeout lands in the plan's device status, and the next
+ * bmfr_plan_check_device returns BMFR_E_TIMEOUT; the plan and the CUDA
+ * context stay usable.  No fault, trap or endless wait is involved. */
+int bmfr_plan_probe_bounded_wait(bmfr_plan* plan, unsigned int limit_us, void* stream);
+
 /* Error text of the last failing call on this thread ("" if none). */
 const char* bmfr_last_error(void);
 const char* bmfr_status_string(int status);
