@@ -1041,8 +1041,8 @@ def main():
     elapsed_ms = max_over_ranks(elapsed_ms, device=dev)   # the slowest rank
     value = world * args.steps / (elapsed_ms / 1e3)
     # noise table, block kernel, taa (fused); noise table, accumulate, fitter,
-    # weighted_sum, accumulate_filtered, taa (staged)
-    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 6
+    # weighted sum + filtered accumulation, taa (staged)
+    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 5
 
     # ---- per-stage profile (same workload, events between stages) ------------
     plan.enable_profiling(True)
