@@ -272,9 +272,11 @@ def batch_scenes(rank):
 
 
 def run_batched(args, world, rank, local, dev, barrier, pg):
-    """Batched form: 24 streams of uneven size, one graph-captured step per
-    frame of every stream, binary16 histories and FP32 QR, autotuned; next to
-    the plain per-frame path on the same streams."""
+    """Batched form: 24 streams of uneven size, one step per frame of every
+    stream (staged: each stream's plan kernels on four worker CUDA streams;
+    fused: one graph-captured launch over all streams' blocks), binary16
+    histories and FP32 QR; next to the plain per-frame path on the same
+    streams."""
     import torch
     import bmfr_b200 as B
     scenes = batch_scenes(rank)
@@ -370,7 +372,10 @@ def run_batched(args, world, rank, local, dev, barrier, pg):
             "plain_path": {"value": plain_value, "unit": "frames/s", "ms_per_round": plain_ms / plain_steps,
                            "how": "one plan per stream, staged pipeline, reference arithmetic, frames in turn"},
             "speedup_vs_plain": value / plain_value / world,
-            "clocks": clocks.summary(), "gpu_launches": 3 * args.steps,
+            # per step: noise table, block kernel, TAA (fused); per stream noise
+            # table, accumulation, fitter, weighted sum + filtered accumulation, TAA (staged)
+            "clocks": clocks.summary(),
+            "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 5 * n) * args.steps,
         }), flush=True)
 
 
@@ -727,8 +732,12 @@ def run_served(args, world, rank, local, dev, barrier, pg):
             "capacity": {"batched": cap_batched, "plain": cap_plain, "ratio": cap_batched / cap_plain,
                          "unit": "frames/s", "streams": len(cap_streams),
                          "how": "every seat's first stream with a frame ready at every step; batched: one "
-                                "graph-captured step per frame of all streams; plain: their plans in turn"},
-            "clocks": clocks.summary(), "gpu_launches": 3 * int(st["steps"]),
+                                "step per frame of all streams (staged: each stream's plan kernels on four "
+                                "worker CUDA streams; fused: one graph-captured block-queue launch); plain: "
+                                "their plans in turn"},
+            # per step: 5 kernels per listed stream (staged) or noise, block kernel, TAA (fused)
+            "clocks": clocks.summary(),
+            "gpu_launches": (5 * int(st.get("frames", 0)) if args.pipeline == "staged" else 3 * int(st["steps"])),
         }), flush=True)
 
 

@@ -91,6 +91,10 @@ size_t stream_bytes(const bmfr_params& p, int w, int h, bool own_inputs) {
 
 }  // namespace
 
+// Worker CUDA streams of the staged step: the listed streams' kernels are
+// spread over them so that the kernels of small streams run side by side.
+constexpr int kStepWorkers = 4;
+
 struct bmfr_batch {
     // Guards the slot table, `used` and `last`: streams may be added and
     // removed from other threads while a step is being formed.
@@ -116,6 +120,11 @@ struct bmfr_batch {
     cudaEvent_t mem_ready = nullptr;
     int next = 0;
     int last = -1;
+    // staged step: workers, the fork and join events, the fitter's status word
+    cudaStream_t workers[kStepWorkers] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kStepWorkers] = {};
+    int* d_status = nullptr;
 };
 
 namespace {
@@ -153,8 +162,9 @@ void destroy_graphs(bmfr_batch* b) {
     b->graphs_valid = false;
 }
 
-// Captures the step: description upload, queue reset, noise tables, the
-// block queue and the TAA tiles.  One graph per pinned description buffer.
+// Captures the fused step: description upload, queue reset, noise tables,
+// the block queue and the TAA tiles.  One graph per pinned description
+// buffer.
 int build_graphs(bmfr_batch* b) {
     for (cudaEvent_t e : b->done)
         if (e) cudaEventSynchronize(e);
@@ -173,14 +183,9 @@ int build_graphs(bmfr_batch* b) {
         e = cudaMemcpyAsync(b->d_desc, b->h_desc[k], sizeof(bmfr::BatchStepDesc), cudaMemcpyHostToDevice, cs);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(int), cs);
         if (e == cudaSuccess) e = bmfr::launch_batch_noise(b->d_desc, BMFR_BATCH_MAX_STREAMS, cs);
-        if (b->p.pipeline == BMFR_PIPELINE_STAGED) {
-            if (e == cudaSuccess) e = bmfr::launch_batch_accumulate(b->d_desc, b->p.half_history != 0, b->sms, cs);
-            if (e == cudaSuccess) e = bmfr::launch_batch_fitter(b->d_desc, b->p.fp32_qr, half_tmp, ctas * b->sms, cs);
-            if (e == cudaSuccess) e = bmfr::launch_batch_wsacc(b->d_desc, b->p.half_history != 0, b->sms, cs);
-        } else if (e == cudaSuccess) {
+        if (e == cudaSuccess)
             e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr, half_tmp,
                                           b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms, cs);
-        }
         if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
         if (e == cudaSuccess) e = e2;
@@ -275,6 +280,63 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
     return BMFR_OK;
 }
 
+// The staged step on the streams of description d (host copy): for each
+// stream the plan's kernels — noise table, accumulation, fitter, weighted sum
+// + filtered accumulation, TAA — with the stream's buffers, the same
+// launches and arithmetic as a plan's frame, so each stream's output equals
+// the plan's.  The streams are spread over the worker CUDA streams, largest
+// first onto the least loaded worker, forked from and joined into `s`.
+cudaError_t launch_staged_step(bmfr_batch* b, const bmfr::BatchStepDesc& d, cudaStream_t s) {
+    const bool half_tmp = b->p.use_half_precision_in_tmp_data != 0;
+    const bool half_hist = b->p.half_history != 0;
+    std::vector<int> order(d.n_streams);
+    for (int i = 0; i < d.n_streams; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return d.s[x].job.g.blocks > d.s[y].job.g.blocks;
+    });
+    long long load[kStepWorkers] = {};
+    bool used[kStepWorkers] = {};
+    cudaError_t e = cudaEventRecord(b->fork, s);
+    for (int i : order) {
+        if (e != cudaSuccess) break;
+        int w = 0;
+        for (int k = 1; k < kStepWorkers; ++k)
+            if (load[k] < load[w]) w = k;
+        const bmfr::BatchStreamJob& J = d.s[i];
+        const bmfr::FusedBuffers& fb = J.job.fb;
+        const bmfr::Geometry& g = J.job.g;
+        const int f = J.job.a.frame;
+        cudaStream_t ws = b->workers[w];
+        if (!used[w]) {
+            e = cudaStreamWaitEvent(ws, b->fork, 0);
+            used[w] = true;
+        }
+        load[w] += g.blocks;
+        if (e == cudaSuccess) e = bmfr::launch_noise_table(f, const_cast<float*>(fb.noise), ws);
+        if (e == cudaSuccess)
+            e = bmfr::launch_accumulate_noisy(g, J.job.a, fb.prev_pix, fb.accept, fb.cur_n, fb.prev_n, fb.cur_p,
+                                              fb.prev_p, fb.noisy_in, fb.noisy_acc_cur, fb.noisy_acc_prev, half_hist,
+                                              fb.prev_spp, fb.cur_spp, J.tmp, ws);
+        if (e == cudaSuccess)
+            e = bmfr::launch_fitter(g, f, J.job.nc, J.tmp, half_tmp, b->p.fp32_qr, fb.weights, fb.mins_maxs,
+                                    fb.noise, b->d_status, ws);
+        if (e == cudaSuccess)
+            e = bmfr::launch_weighted_sum_accumulate(g, f, J.job.second_alpha, fb.weights, fb.mins_maxs, fb.cur_n,
+                                                     fb.cur_p, nullptr, fb.prev_pix, fb.accept, fb.albedo,
+                                                     fb.tone_mapped, fb.cur_spp, fb.acc_prev, fb.acc_cur, half_hist,
+                                                     ws);
+        if (e == cudaSuccess)
+            e = bmfr::launch_taa(g, f, J.taa_alpha, fb.prev_pix, fb.tone_mapped, J.result_hist, J.result_prev,
+                                 J.result_out, half_hist, ws);
+    }
+    for (int w = 0; w < kStepWorkers && e == cudaSuccess; ++w) {
+        if (!used[w]) continue;
+        e = cudaEventRecord(b->join[w], b->workers[w]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->join[w], 0);
+    }
+    return e;
+}
+
 }  // namespace
 
 extern "C" {
@@ -305,9 +367,16 @@ int bmfr_batch_create(const bmfr_params* params, size_t memory_budget_bytes, bmf
     const bool half_tmp = params->use_half_precision_in_tmp_data != 0;
     b->block_occupancy =
         std::max(1, params->pipeline == BMFR_PIPELINE_STAGED
-                        ? bmfr::batch_fitter_occupancy(params->fp32_qr, half_tmp)
+                        ? 1
                         : bmfr::batch_block_occupancy(params->fp32_qr, half_tmp, params->half_history != 0));
     cudaError_t e = cudaMalloc(&b->d_desc, sizeof(bmfr::BatchStepDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int w = 0; w < kStepWorkers && e == cudaSuccess; ++w) {
+        e = cudaStreamCreateWithFlags(&b->workers[w], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[w], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * sizeof(int));
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         e = cudaMallocHost(&b->h_desc[k], sizeof(bmfr::BatchStepDesc));
@@ -352,6 +421,13 @@ int bmfr_batch_destroy(bmfr_batch* b) {
     if (b->mem_ready) cudaEventDestroy(b->mem_ready);
     if (b->mem_stream) cudaStreamDestroy(b->mem_stream);
     if (b->pool) cudaMemPoolDestroy(b->pool);
+    for (int w = 0; w < kStepWorkers; ++w) {
+        if (b->workers[w]) cudaStreamSynchronize(b->workers[w]);
+        if (b->workers[w]) cudaStreamDestroy(b->workers[w]);
+        if (b->join[w]) cudaEventDestroy(b->join[w]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->d_status) cudaFree(b->d_status);
     if (b->d_desc) cudaFree(b->d_desc);
     if (b->d_counters) cudaFree(b->d_counters);
     delete b;
@@ -470,7 +546,8 @@ int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io*
     if (int st = check_batch(b)) return st;
     if (n <= 0 || n > BMFR_BATCH_MAX_STREAMS || !slots || !matrices || !offsets)
         return fail(BMFR_E_INVALID, "step: bad stream list");
-    if (!b->graphs_valid)
+    const bool staged = b->p.pipeline == BMFR_PIPELINE_STAGED;
+    if (!staged && !b->graphs_valid)
         if (int st = build_graphs(b)) return st;
     const int k = b->next;
     cudaError_t e = cudaEventSynchronize(b->done[k]);   // description buffer k is free again
@@ -489,9 +566,9 @@ int bmfr_batch_step(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io*
     }
     e = cudaStreamWaitEvent(s, b->mem_ready, 0);   // streams added since are allocated and zeroed
     if (e != cudaSuccess) return cuda_fail(e, "step: ordering after stream allocation");
-    e = cudaGraphLaunch(b->graph[k], s);
+    e = staged ? launch_staged_step(b, *b->h_desc[k], s) : cudaGraphLaunch(b->graph[k], s);
     if (e == cudaSuccess) e = cudaEventRecord(b->done[k], s);
-    if (e != cudaSuccess) return cuda_fail(e, "step: graph launch");
+    if (e != cudaSuccess) return cuda_fail(e, staged ? "step: launches" : "step: graph launch");
     b->last = k;
     b->next = k ^ 1;
     for (int i = 0; i < n; ++i) b->slots[slots[i]].frame += 1;
@@ -651,7 +728,7 @@ int bmfr_batch_set_tuning(bmfr_batch* b, const bmfr_batch_tuning* t) {
     b->tuning.tile_w = t->taa_tile_w;
     b->tuning.tile_h = t->taa_tile_h;
     b->tuning.staging_depth = t->staging_depth;
-    return build_graphs(b);
+    return b->p.pipeline == BMFR_PIPELINE_STAGED ? BMFR_OK : build_graphs(b);   // the staged step has no graph
 }
 
 int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame_io* io, const float* matrices,
@@ -678,6 +755,17 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
     bmfr_batch_tuning best{0, 30, 32, 0};
     float best_t = 1e30f;
     int status = BMFR_OK;
+    if (b->p.pipeline == BMFR_PIPELINE_STAGED) {
+        // The staged step launches the plan's kernels, whose shapes are
+        // fixed: only its time is reported.
+        status = time_tuning(best, &best_t);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (status != BMFR_OK) return status;
+        if (chosen) *chosen = best;
+        if (best_ms) *best_ms = best_t;
+        return BMFR_OK;
+    }
     // Blocks per SM and staging depth together, then the TAA CTA shape.
     for (int ctas = 1; ctas <= b->block_occupancy && status == BMFR_OK; ++ctas) {
         const int max_depth = b->p.pipeline == BMFR_PIPELINE_STAGED ? 0 : 2;   // staging: fused step only

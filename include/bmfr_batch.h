@@ -3,14 +3,17 @@
  * The reference denoises one stream on one in-order queue
  * (opencl/bmfr.cpp:191, 417-485); this layer has no counterpart there.  A
  * batch holds the temporal history of many streams of uneven resolution in
- * HBM and denoises one frame of any subset of them per step, as one CUDA
- * graph: with params.pipeline = BMFR_PIPELINE_FUSED the step's 32x32 blocks
- * of all those streams form one queue that a single persistent launch of the
- * fused block kernel walks; with BMFR_PIPELINE_STAGED persistent launches
- * walk all streams' margin tiles (accumulation), blocks (fitter) and image
- * tiles (weighted sum and filtered accumulation).  TAA follows in one more
- * launch.  Each stream's result is exactly what a plan with the same
- * parameters (pipeline included) produces for it alone.
+ * HBM and denoises one frame of any subset of them per step.  With
+ * params.pipeline = BMFR_PIPELINE_FUSED the step is one CUDA graph: the
+ * step's 32x32 blocks of all those streams form one queue that a single
+ * persistent launch of the fused block kernel walks, and TAA follows in one
+ * more launch.  With BMFR_PIPELINE_STAGED each listed stream runs a plan's
+ * kernels (noise table, accumulation, fitter, weighted sum + filtered
+ * accumulation, TAA) on its own buffers, the streams spread over four worker
+ * CUDA streams forked from and joined into the caller's stream, so that the
+ * kernels of different streams overlap.  Each stream's result is exactly
+ * what a plan with the same parameters (pipeline included) produces for it
+ * alone.
  *
  * A server on top admits render streams against a memory budget, queues
  * their frame requests as they arrive and runs steps continuously, so that
@@ -41,13 +44,14 @@ typedef struct bmfr_batch bmfr_batch;
 
 /* Launch parameters of a step, chosen by bmfr_batch_autotune. */
 typedef struct bmfr_batch_tuning {
-    int block_ctas_per_sm;  /* persistent CTAs of the block kernel (fused) or fitter (staged) per SM
+    int block_ctas_per_sm;  /* fused step: persistent CTAs of the block kernel per SM
                                (0: as many as fit) */
-    int taa_tile_w;         /* TAA CTA tile: 30 columns x 16, 32 or 64 rows */
+    int taa_tile_w;         /* fused step's TAA CTA tile: 30 columns x 16, 32 or 64 rows */
     int taa_tile_h;
     int staging_depth;      /* fused step: 0 takes blocks from an atomic queue; k > 0 a static
                                order with the inputs of each CTA's next k blocks prefetched
-                               into L2.  The staged step double-buffers its fitter tiles. */
+                               into L2.  The staged step launches a plan's kernels, whose
+                               shapes are fixed: it has nothing to tune. */
 } bmfr_batch_tuning;
 
 /* memory_budget_bytes: device bytes the batch's streams may hold (0: no limit).
@@ -108,7 +112,8 @@ int bmfr_batch_get_tuning(const bmfr_batch* batch, bmfr_batch_tuning* tuning);
 int bmfr_batch_set_tuning(bmfr_batch* batch, const bmfr_batch_tuning* tuning);
 /* Times candidate tunings on `steps` steps of the given work (which advances
  * the listed streams' histories; reset them afterwards if that matters),
- * keeps the fastest and returns it with its mean step time. */
+ * keeps the fastest and returns it with its mean step time (staged step:
+ * only its time; the tuning stays as it is). */
 int bmfr_batch_autotune(bmfr_batch* batch, int n, const int* slots, const bmfr_frame_io* io,
                         const float* matrices, const float* offsets, int steps, void* stream,
                         bmfr_batch_tuning* chosen, float* best_ms);
