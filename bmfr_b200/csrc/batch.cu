@@ -1,15 +1,12 @@
 // batch.cu — kernels of the many-stream engine (batched and served forms).
 //
-// One step denoises one frame of every participating stream.  In the fused
-// step the streams' 32x32 blocks form one global queue that a single
-// persistent launch of the fused block kernel walks (accumulate + fit +
-// weighted sum + filtered accumulation per block, fused_block.cuh); in the
-// staged step three persistent launches walk all streams' margin tiles
-// (accumulation into each stream's tmp_data), their blocks (the fitter, tile
-// by bulk TMA copy, two buffers) and their image tiles (weighted sum +
-// filtered accumulation).  A last launch walks the streams' TAA tiles.  All
-// read the step's description from device memory, so one captured CUDA
-// graph serves every step.
+// The fused step: one frame of every participating stream, the streams'
+// 32x32 blocks forming one global queue that a single persistent launch of
+// the fused block kernel walks (accumulate + fit + weighted sum + filtered
+// accumulation per block, fused_block.cuh), then one launch over the
+// streams' TAA tiles.  Both read the step's description from device memory,
+// so one captured CUDA graph serves every step.  (The staged step runs the
+// plan's kernels per stream, batch_host.cu.)
 #include <type_traits>
 
 #include "batch.cuh"
@@ -35,19 +32,6 @@ __device__ __forceinline__ int stream_of_tile(const BatchStepDesc* __restrict__ 
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (d->s[mid].tile_start <= tile) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-// Stream whose range of a step queue holds `item`, by binary search on the
-// streams' first indices (member `first` of BatchStreamJob).
-template <int BatchStreamJob::*first>
-__device__ __forceinline__ int stream_of(const BatchStepDesc* __restrict__ d, int item) {
-    int lo = 0, hi = d->n_streams - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (d->s[mid].*first <= item) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -127,116 +111,6 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
     }
 }
 
-// ---- staged step ----------------------------------------------------------
-
-template <typename HistT>
-__global__ void __launch_bounds__(256) k_batch_accumulate(const BatchStepDesc* __restrict__ d) {
-    const int nt = d->n_acc_tiles;
-    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-        const int s = stream_of<&BatchStreamJob::acc_tile_start>(d, tile);
-        const BatchStreamJob& J = d->s[s];
-        const Geometry& g = J.job.g;
-        const FusedBuffers& fb = J.job.fb;
-        const int t = tile - J.acc_tile_start, tx = g.MW / 32;
-        const int gx = (t % tx) * 32 + (int)(threadIdx.x & 31), gy = (t / tx) * 8 + (int)(threadIdx.x >> 5);
-        accumulate_margin_px<HistT>(g, J.job.a, gx, gy, fb.prev_pix, fb.accept, fb.cur_n, fb.prev_n, fb.cur_p,
-                                    fb.prev_p, fb.noisy_in, (HistT*)fb.noisy_acc_cur, (const HistT*)fb.noisy_acc_prev,
-                                    fb.prev_spp, fb.cur_spp, J.tmp);
-    }
-}
-
-template <bool HALF_TMP>
-struct BatchFitterShared {
-    using TmpT = typename std::conditional<HALF_TMP, __half, float>::type;
-    alignas(128) TmpT tile[2][kBuffers * kBlockPixels];
-    FitterSmem sm;
-    alignas(8) uint64_t bar[2];
-};
-
-// The fitter over the step's block queue: persistent CTAs, each block's
-// tmp_data by one bulk copy, the copy of the block after next in flight
-// while the current one is fitted; waits are bounded as in the standalone
-// fitter (a timeout stops the CTA; the step's results are then undefined).
-template <int METHOD, bool HALF_TMP>
-__global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2)
-    k_batch_fitter(const BatchStepDesc* __restrict__ d) {
-    using Shared = BatchFitterShared<HALF_TMP>;
-    using TmpT = typename Shared::TmpT;
-    constexpr bool ROUND = HALF_TMP && METHOD == kFitReference;
-    constexpr uint32_t kTileBytes = kBuffers * kBlockPixels * sizeof(TmpT);
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    Shared& S = *reinterpret_cast<Shared*>(smem_raw);
-    const int nb = d->n_blocks;
-    const int id = work_item_id();
-    auto issue = [&](int stage, int item) {
-        const int s = stream_of<&BatchStreamJob::block_start>(d, item);
-        const char* src = static_cast<const char*>(d->s[s].tmp) + (size_t)(item - d->s[s].block_start) * kTileBytes;
-        mbar_arrive_expect_tx(&S.bar[stage], kTileBytes);
-        bulk_copy_g2s(S.tile[stage], src, kTileBytes, &S.bar[stage]);
-    };
-    if (threadIdx.x == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
-        fence_barrier_init();
-        S.sm.status = 0;
-        for (int st = 0; st < 2; ++st)
-            if (blockIdx.x + st * (int)gridDim.x < nb) issue(st, blockIdx.x + st * gridDim.x);
-    }
-    __syncthreads();
-    int it = 0;
-    for (int item = blockIdx.x; item < nb; item += gridDim.x, ++it) {
-        const int st = it & 1;
-        const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-        if (threadIdx.x == 0 && !mbar_wait_bounded(&S.bar[st], phase)) S.sm.status = kDevTimeout;
-        __syncthreads();
-        if (S.sm.status) {
-            if (threadIdx.x == 0)
-                for (int k = 0; k < 2; ++k)
-                    if (item + k * (int)gridDim.x < nb) mbar_wait_bounded(&S.bar[(it + k) & 1], (uint32_t)((it + k) >> 1) & 1u);
-            return;
-        }
-        Tile<ROUND> t;
-#pragma unroll
-        for (int k = 0; k < kBuffers; ++k) {
-            const TmpT* col = S.tile[st] + k * kBlockPixels + id;
-            if constexpr (ROUND) {
-                t.h[k][0] = __halves2half2(col[0], col[kLocal]);
-                t.h[k][1] = __halves2half2(col[2 * kLocal], col[3 * kLocal]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if constexpr (HALF_TMP) t.set1(k, q, __half2float(col[q * kLocal]));
-                    else t.set1(k, q, col[q * kLocal]);
-                }
-            }
-        }
-        __syncthreads();   // the buffer is free again
-        const int next = item + 2 * (int)gridDim.x;
-        if (threadIdx.x == 0 && next < nb) issue(st, next);
-        const int s = stream_of<&BatchStreamJob::block_start>(d, item);
-        const BlockJob& j = d->s[s].job;
-        const int b = item - d->s[s].block_start;
-        fit_block<ROUND, METHOD>(t, j.fb.noise, j.nc, S.sm, j.fb.weights + (size_t)b * kFeatures * 3,
-                                 j.fb.mins_maxs + (size_t)b * kScaled * 2);
-    }
-}
-
-template <typename HistT>
-__global__ void __launch_bounds__(256) k_batch_wsacc(const BatchStepDesc* __restrict__ d) {
-    const int nt = d->n_px_tiles;
-    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-        const int s = stream_of<&BatchStreamJob::px_tile_start>(d, tile);
-        const BatchStreamJob& J = d->s[s];
-        const Geometry& g = J.job.g;
-        const FusedBuffers& fb = J.job.fb;
-        const int t = tile - J.px_tile_start, tx = (g.W + 31) / 32;
-        const int px = (t % tx) * 32 + (int)(threadIdx.x & 31), py = (t / tx) * 8 + (int)(threadIdx.x >> 5);
-        if (px < g.W && py < g.H)
-            wsacc_px<HistT>(g, J.job.a.frame, J.job.second_alpha, px, py, fb.weights, fb.mins_maxs, fb.cur_n, fb.cur_p,
-                            nullptr, fb.prev_pix, fb.accept, fb.albedo, fb.tone_mapped, fb.cur_spp,
-                            (const HistT*)fb.acc_prev, (HistT*)fb.acc_cur);
-    }
-}
 
 // TAA tiles of 30 columns x 4R rows: four warps per CTA, R rows each
 // (taa_strip).
@@ -308,63 +182,6 @@ int batch_block_occupancy(int qr, bool half_tmp, bool half_history) {
     return dispatch_blocks<float>(qr, half_tmp, Occupancy{});
 }
 
-cudaError_t launch_batch_accumulate(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
-    if (half_history) k_batch_accumulate<__half><<<sms * 8, 256, 0, s>>>(desc);
-    else k_batch_accumulate<float><<<sms * 8, 256, 0, s>>>(desc);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_batch_wsacc(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
-    if (half_history) k_batch_wsacc<__half><<<sms * 8, 256, 0, s>>>(desc);
-    else k_batch_wsacc<float><<<sms * 8, 256, 0, s>>>(desc);
-    return cudaGetLastError();
-}
-
-template <int METHOD, bool HALF_TMP>
-static int fitter_smem() {
-    return (int)sizeof(BatchFitterShared<HALF_TMP>);
-}
-
-// The fitter instance for (qr, half_tmp) handed to F::run.
-template <typename F>
-static auto dispatch_fitter(int qr, bool half_tmp, F&& f) {
-    if (!half_tmp) return f.template run<kFitReference, false>();
-    if (qr == kFitCholQR2) return f.template run<kFitCholQR2, true>();
-    if (qr == kFitHouseholder32) return f.template run<kFitHouseholder32, true>();
-    return f.template run<kFitReference, true>();
-}
-
-struct LaunchFitter {
-    const BatchStepDesc* desc;
-    int grid;
-    cudaStream_t s;
-    template <int M, bool H>
-    cudaError_t run() const {
-        k_batch_fitter<M, H><<<grid, kLocal, fitter_smem<M, H>(), s>>>(desc);
-        return cudaGetLastError();
-    }
-};
-
-struct FitterOccupancy {
-    template <int M, bool H>
-    int run() const {
-        const int smem = fitter_smem<M, H>();
-        if (cudaFuncSetAttribute(k_batch_fitter<M, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess)
-            return 1;
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_fitter<M, H>, kLocal, smem);
-        return per_sm;
-    }
-};
-
-// batch_fitter_occupancy (called when the batch is created) also raises the
-// kernel's shared-memory limit, which the launch needs.
-cudaError_t launch_batch_fitter(const BatchStepDesc* desc, int qr, bool half_tmp, int grid, cudaStream_t s) {
-    return dispatch_fitter(qr, half_tmp, LaunchFitter{desc, grid, s});
-}
-
-int batch_fitter_occupancy(int qr, bool half_tmp) { return dispatch_fitter(qr, half_tmp, FitterOccupancy{}); }
 
 template <int R>
 static cudaError_t launch_taa_t(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {

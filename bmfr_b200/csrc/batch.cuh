@@ -20,15 +20,11 @@ struct BatchStreamJob {
     void* result_hist;         // TAA history written this frame (float or binary16)
     const void* result_prev;   // TAA history of the previous frame
     float* result_out;         // optional float copy of the output
-    // staged step only
-    void* tmp;                 // the stream's tmp_data
-    int acc_tile_start;        // first 32x8 margin tile of this stream (accumulation)
-    int px_tile_start;         // first 32x8 image tile of this stream (weighted sum + filtered accumulation)
+    void* tmp;                 // the stream's tmp_data (staged step)
 };
 
 struct BatchStepDesc {
     int n_streams, n_blocks, n_tiles, tile_w;
-    int n_acc_tiles, n_px_tiles;
     BatchStreamJob s[kBatchMaxStreams];
 };
 
@@ -49,13 +45,5 @@ cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const
                              cudaStream_t s);
 int batch_block_occupancy(int qr, bool half_tmp, bool half_history);
 
-// The staged step: accumulation over every stream's margin tiles (writing
-// each stream's tmp_data), the fitter over the step's block queue (grid:
-// persistent CTAs, batch_fitter_occupancy per SM), weighted sum + filtered
-// accumulation over the image tiles; then launch_batch_taa.
-cudaError_t launch_batch_accumulate(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s);
-cudaError_t launch_batch_fitter(const BatchStepDesc* desc, int qr, bool half_tmp, int grid, cudaStream_t s);
-cudaError_t launch_batch_wsacc(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s);
-int batch_fitter_occupancy(int qr, bool half_tmp);
 
 }  // namespace bmfr

@@ -218,7 +218,7 @@ bmfr::AccumArgs step_args(const bmfr_batch* b, const float* m, const float* off,
 int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, const bmfr_frame_io* io,
               const float* matrices, const float* offsets) {
     const int tw = b->tuning.tile_w, th = b->tuning.tile_h;
-    int blocks = 0, tiles = 0, acc_tiles = 0, px_tiles = 0;
+    int blocks = 0, tiles = 0;
     for (int i = 0; i < n; ++i) {
         StreamSlot& s = b->slots[slots[i]];
         const int f = s.frame, cur = f & 1, prv = cur ^ 1;
@@ -264,15 +264,9 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
         J.result_prev = s.result[prv];
         J.result_out = (fi && fi->result) ? fi->result : s.result_f32;
         J.tmp = s.tmp;
-        J.acc_tile_start = acc_tiles;
-        J.px_tile_start = px_tiles;
         blocks += s.g.blocks;
         tiles += J.tiles_x * ((s.height + th - 1) / th);
-        acc_tiles += (s.g.MW / 32) * (s.g.MH / 8);
-        px_tiles += ((s.width + 31) / 32) * ((s.height + 7) / 8);
     }
-    d->n_acc_tiles = acc_tiles;
-    d->n_px_tiles = px_tiles;
     d->n_streams = n;
     d->n_blocks = blocks;
     d->n_tiles = tiles;
