@@ -273,7 +273,7 @@ def batch_scenes(rank):
 
 def run_batched(args, world, rank, local, dev, barrier, pg):
     """Batched form: 24 streams of uneven size, one step per frame of every
-    stream (staged: each stream's plan kernels on four worker CUDA streams;
+    stream (staged: each stream's plan kernels on eight worker CUDA streams;
     fused: one graph-captured launch over all streams' blocks), binary16
     histories and FP32 QR; next to the plain per-frame path on the same
     streams."""
@@ -732,7 +732,7 @@ def run_served(args, world, rank, local, dev, barrier, pg):
             "capacity": {"batched": cap_batched, "plain": cap_plain, "ratio": cap_batched / cap_plain,
                          "unit": "frames/s", "streams": len(cap_streams),
                          "how": "every seat's first stream with a frame ready at every step; batched: one "
-                                "step per frame of all streams (staged: each stream's plan kernels on four "
+                                "step per frame of all streams (staged: each stream's plan kernels on eight "
                                 "worker CUDA streams; fused: one graph-captured block-queue launch); plain: "
                                 "their plans in turn"},
             # per step: 5 kernels per listed stream (staged) or noise, block kernel, TAA (fused)

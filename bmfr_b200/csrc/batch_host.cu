@@ -93,7 +93,7 @@ size_t stream_bytes(const bmfr_params& p, int w, int h, bool own_inputs) {
 
 // Worker CUDA streams of the staged step: the listed streams' kernels are
 // spread over them so that the kernels of small streams run side by side.
-constexpr int kStepWorkers = 4;
+constexpr int kStepWorkers = 8;
 
 struct bmfr_batch {
     // Guards the slot table, `used` and `last`: streams may be added and

@@ -9,7 +9,7 @@
  * persistent launch of the fused block kernel walks, and TAA follows in one
  * more launch.  With BMFR_PIPELINE_STAGED each listed stream runs a plan's
  * kernels (noise table, accumulation, fitter, weighted sum + filtered
- * accumulation, TAA) on its own buffers, the streams spread over four worker
+ * accumulation, TAA) on its own buffers, the streams spread over eight worker
  * CUDA streams forked from and joined into the caller's stream, so that the
  * kernels of different streams overlap.  Each stream's result is exactly
  * what a plan with the same parameters (pipeline included) produces for it
