@@ -318,7 +318,8 @@ def taa(plan: Plan, in_prev_frame_pixel, new_frame, result_frame, prev_frame, fr
 # -- many streams (include/bmfr_batch.h) -------------------------------------
 
 class Batch:
-    """Many streams of uneven size denoised together, one CUDA graph per step."""
+    """Many streams of uneven size denoised together, one step per frame of any
+    subset of them (see include/bmfr_batch.h for the fused and staged steps)."""
 
     def __init__(self, params: Params | None = None, memory_budget_bytes: int = 0, **overrides):
         self.params = params if params is not None else default_params(**overrides)
@@ -413,7 +414,9 @@ class Batch:
         return n, sl, iop, (m, o), mp, op
 
     def step(self, slots, matrices, offsets, io=None, stream=None) -> None:
-        """Denoises the next frame of each stream in `slots` (one graph launch)."""
+        """Denoises the next frame of each stream in `slots`: one graph launch
+        (fused step) or each stream's plan kernels on the batch's worker
+        streams, joined into `stream` (staged step)."""
         n, sl, iop, keep, mp, op = self._args(slots, io, matrices, offsets)
         check(lib.bmfr_batch_step(self.handle, n, sl, iop, mp, op, _stream_ptr(stream)), "bmfr_batch_step")
 

@@ -43,6 +43,11 @@ class Stream:
         return out
 
 
+def _cudart():
+    from test_parity_pipeline import _cudart as cudart
+    return cudart()
+
+
 def _device_result(ptr, w, h):
     import torch
     from test_parity_pipeline import device_array
@@ -72,6 +77,42 @@ def test_batch_equals_streams_alone(cuda, qr, pipeline):
             np.testing.assert_array_equal(got, want, err_msg=f"stream {i} frame {frame[i]}")
             frame[i] += 1
             assert batch.frame(slots[i]) == frame[i]
+    torch.cuda.synchronize()
+    batch.close()
+
+
+def test_staged_step_with_more_streams_than_workers(cuda):
+    """Twelve streams (more than the staged step's worker CUDA streams, so a
+    worker runs several streams' kernels in turn), all of them, then a
+    subset in another order, then all again: every result equals its plan's
+    bit for bit, and the whole step is complete when the caller's stream is."""
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_STAGED, fp32_qr=B.QR_CHOLESKY2, half_history=1)
+    sizes = [SIZES[k % len(SIZES)] for k in range(12)]
+    streams = [Stream(20 + k, w, h, params, cuda) for k, (w, h) in enumerate(sizes)]
+    batch = B.Batch(params)
+    slots = [batch.add_stream(s.w, s.h) for s in streams]
+    caller = torch.cuda.Stream(device=cuda)
+    schedule = [list(range(12)), [11, 3, 7, 0, 5], list(range(12))]
+    frame = [0] * len(streams)
+    for active in schedule:
+        io = [streams[i].io(frame[i]) for i in active]
+        mats = np.concatenate([streams[i].sc.prev_camera(frame[i]) for i in active])
+        offs = np.concatenate([streams[i].sc.pixel_offset(frame[i]) for i in active])
+        batch.step([slots[i] for i in active], mats, offs, io=io, stream=caller)
+        caller.synchronize()
+        # Read without a device-wide synchronisation: the worker streams are
+        # non-blocking, so only the step's join into `caller` orders them
+        # before this copy.
+        got = {}
+        for i in active:
+            out = np.empty((streams[i].h, streams[i].w, 3), np.float32)
+            assert _cudart().cudaMemcpy(out.ctypes.data, batch.result_ptr(slots[i]), out.nbytes, 2) == 0
+            got[i] = out
+        for i in active:
+            want = streams[i].plan_step(frame[i]).cpu().numpy().reshape(streams[i].h, streams[i].w, 3)
+            np.testing.assert_array_equal(got[i], want, err_msg=f"stream {i} frame {frame[i]}")
+            frame[i] += 1
     torch.cuda.synchronize()
     batch.close()
 
