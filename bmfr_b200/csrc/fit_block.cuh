@@ -244,6 +244,15 @@ __device__ __forceinline__ void fill_noise_table(float* table, int frame) {
 // each rounded exactly as the scalar form, in one instruction.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// Products that must round on their own: a packed multiply whose result
+// feeds a packed add is fused into one packed fused multiply-add by the
+// compiler (measured: the reference-arithmetic fitter then differed from the
+// reference in the last bits of most weights with float32 tmp_data, and of
+// ~1 % with binary16), while a scalar __fmul_rn is never contracted.  The
+// reference-arithmetic path and the noise term use these.
+__device__ __forceinline__ float2 rmul2(float2 a, float2 b) {
+    return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
@@ -251,7 +260,7 @@ __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 // add_noise_r on two values at once.
 __device__ __forceinline__ float2 add_noise_r2(float2 v, float2 r, NoiseConst c) {
     const float2 hi = dup2(c.hi), lo = dup2(c.lo);
-    const float2 p = mul2(hi, r);
+    const float2 p = rmul2(hi, r);
     const float2 pe = fma2(hi, r, neg2(p));
     const float2 pl = fma2(lo, r, pe);
     const float2 sm = add2(v, p);
@@ -318,10 +327,10 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             float2 a01, a23, b01, b23;
             load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
             load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
-            float2 s = add2(dup2(0.0f), mul2(make_float2(a01.x, b01.x), uq0));
-            s = add2(s, mul2(make_float2(a01.y, b01.y), uq1));
-            s = add2(s, mul2(make_float2(a23.x, b23.x), uq2));
-            s = add2(s, mul2(make_float2(a23.y, b23.y), uq3));
+            float2 s = add2(dup2(0.0f), rmul2(make_float2(a01.x, b01.x), uq0));
+            s = add2(s, rmul2(make_float2(a01.y, b01.y), uq1));
+            s = add2(s, rmul2(make_float2(a23.x, b23.x), uq2));
+            s = add2(s, rmul2(make_float2(a23.y, b23.y), uq3));
             d[i] = s.x;
             d[i + 1] = s.y;
         }
@@ -354,8 +363,8 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             float2 n01, n23;
             if (fast) {
                 const float2 d2 = dup2(dot);
-                const float2 num01 = mul2(u2_01, d2), num23 = mul2(u2_23, d2);
-                const float2 nq01 = mul2(num01, ny), nq23 = mul2(num23, ny);
+                const float2 num01 = rmul2(u2_01, d2), num23 = rmul2(u2_23, d2);
+                const float2 nq01 = rmul2(num01, ny), nq23 = rmul2(num23, ny);
                 const float2 r01 = fma2(nq01, b2, num01), r23 = fma2(nq23, b2, num23);
                 n01 = add2(a01, fma2(r01, ny, nq01));
                 n23 = add2(a23, fma2(r23, ny, nq23));

@@ -1,5 +1,5 @@
-"""Writes the reference fixtures tests/golden/ref_pipeline.npz and
-tests/golden/ref_stages.npz.
+"""Writes the reference fixtures tests/golden/ref_pipeline.npz,
+tests/golden/ref_pipeline_f32.npz and tests/golden/ref_stages.npz.
 
 The outputs come from the reference's own OpenCL kernels (opencl/bmfr.cl),
 compiled for the CPU by oracle/ref_cl (oracle.ref.RefKernels), run on the
@@ -31,16 +31,20 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def run_pipeline():
+def run_pipeline(use_half=True):
+    """The scene frames through the reference's kernels; with use_half=False
+    (tmp_data in float32, the reference's USE_HALF_PRECISION_IN_TMP_DATA=0)
+    only the outputs are kept: the inputs are ref_pipeline.npz's."""
     frames, pos_lim, nrm_lim = cases.pipeline_inputs()
     w, h = cases.PIPELINE_SIZE
-    pipe = OraclePipeline(RefKernels(w, h, pos_lim, nrm_lim))
+    pipe = OraclePipeline(RefKernels(w, h, pos_lim, nrm_lim, use_half=use_half))
     out = {"limits": np.array([pos_lim, nrm_lim], np.float32)}
     for f, d in enumerate(frames):
         res = pipe.step(d["albedo"], d["normals"], d["positions"], d["noisy"], d["matrix"], d["offset"])
         c = f & 1
-        for k in ("albedo", "normals", "positions", "noisy", "matrix", "offset"):
-            out[f"in{f}_{k}"] = d[k]
+        if use_half:
+            for k in ("albedo", "normals", "positions", "noisy", "matrix", "offset"):
+                out[f"in{f}_{k}"] = d[k]
         out[f"out{f}_result"] = res.copy()
         out[f"out{f}_tone_mapped"] = pipe.tone_mapped.copy()
         out[f"out{f}_weights"] = pipe.weights.copy()
@@ -49,7 +53,7 @@ def run_pipeline():
         out[f"out{f}_spp"] = pipe.spp[c].copy()
         out[f"out{f}_prev_pix"] = pipe.prev_pix.copy()
         out[f"out{f}_noisy_acc"] = pipe.noisy[c].copy()
-        out[f"sha{f}_tmp"] = np.array(sha(pipe.tmp_after_accumulate.view(np.uint16)))
+        out[f"sha{f}_tmp"] = np.array(sha(pipe.tmp_after_accumulate.view(np.uint16 if use_half else np.uint32)))
         out[f"sha{f}_filtered"] = np.array(sha(pipe.filtered))
         out[f"sha{f}_acc"] = np.array(sha(pipe.acc[c]))
     return out
@@ -98,7 +102,8 @@ def run_stages():
 
 
 def main():
-    for name, fn in (("ref_pipeline.npz", run_pipeline), ("ref_stages.npz", run_stages)):
+    for name, fn in (("ref_pipeline.npz", run_pipeline), ("ref_pipeline_f32.npz", lambda: run_pipeline(False)),
+                     ("ref_stages.npz", run_stages)):
         data = fn()
         np.savez_compressed(HERE / name, **data)
         print(f"{name}: {(HERE / name).stat().st_size / 1024:.0f} KiB, {len(data)} arrays")

@@ -2,14 +2,14 @@
 
 tests/golden/ref_*.npz hold outputs of the reference's OpenCL kernels
 (opencl/bmfr.cl compiled for the CPU, tests/golden/make_golden.py) with the
-inputs that produced them: a three-frame run of the procedural scene, and one
-frame of edge inputs for every stage (NaN, infinities, values beyond
+inputs that produced them: a three-frame run of the procedural scene (with
+binary16 and with float32 tmp_data), and one frame of edge inputs for every
+stage (NaN, infinities, values beyond
 binary16, spp 0 and 255, degenerate blocks, reprojections on and beyond the
 image edges).  The plan pipeline (staged and fused) and the five drop-in
-entry points are run on the stored inputs.  Integer outputs, tmp_data and the
-accumulations must be bit-identical (NaN equal to NaN); the fitted weights
-bit-identical in more than 99 % of values (the noise term, see the fitter);
-tone mapping (powr on the special function unit) and TAA within 1e-5.
+entry points are run on the stored inputs.  Integer outputs, tmp_data, the
+fitted weights and the accumulations must be bit-identical (NaN equal to
+NaN); tone mapping (powr on the special function unit) and TAA within 1e-5.
 """
 from pathlib import Path
 
@@ -34,24 +34,24 @@ def same(a, b, what):
 
 
 def weights_match(got, want, what):
-    got, want = np.asarray(got), np.asarray(want)
-    assert (np.isnan(got) == np.isnan(want)).all(), f"{what}: NaN pattern differs"
-    fin = ~np.isnan(want)
-    exact = (got[fin] == want[fin]).mean()
-    assert exact > 0.99, f"{what}: bit-identical fraction {exact:.4f}"
+    same(got, want, what)
 
 
+@pytest.mark.parametrize("fixture,use_half", [("ref_pipeline.npz", 1), ("ref_pipeline_f32.npz", 0)])
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
-def test_plan_pipeline_matches_reference_fixture(cuda, pipeline):
-    g = np.load(GOLDEN / "ref_pipeline.npz")
+def test_plan_pipeline_matches_reference_fixture(cuda, pipeline, fixture, use_half):
+    """tmp_data in binary16 (the reference's default) and in float32 (its
+    USE_HALF_PRECISION_IN_TMP_DATA=0), on the same scene frames."""
+    inp = np.load(GOLDEN / "ref_pipeline.npz")
+    g = np.load(GOLDEN / fixture)
     frames = sum(1 for k in g.files if k.endswith("_result"))
-    H, W = g["in0_albedo"].shape[:2]
+    H, W = inp["in0_albedo"].shape[:2]
     lim = g["limits"]
     plan = B.Plan(W, H, pipeline=pipeline, position_limit_squared=float(lim[0]),
-                  normal_limit_squared=float(lim[1]))
+                  normal_limit_squared=float(lim[1]), use_half_precision_in_tmp_data=use_half)
     for f in range(frames):
-        plan.upload_frame(g[f"in{f}_albedo"], g[f"in{f}_normals"], g[f"in{f}_positions"], g[f"in{f}_noisy"])
-        plan.denoise_frame(g[f"in{f}_matrix"], g[f"in{f}_offset"])
+        plan.upload_frame(inp[f"in{f}_albedo"], inp[f"in{f}_normals"], inp[f"in{f}_positions"], inp[f"in{f}_noisy"])
+        plan.denoise_frame(inp[f"in{f}_matrix"], inp[f"in{f}_offset"])
         got = plan.download_result()
         bufs = plan.buffers()
         same(device_array(bufs.accept, (H, W), np.uint8), g[f"out{f}_accept"], f"accept {f}")

@@ -15,9 +15,9 @@ from oracle.oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 # Float tolerance: |cuda - oracle| <= RTOL * max(|oracle|, FLOOR).  The CUDA
-# kernels keep the reference's operation order, so most values are
-# bit-identical; pow() in the tone map and the float-float noise term of the
-# fitter may differ in the last bits.
+# kernels keep the reference's operation order, so the fit and the
+# accumulations are bit-identical; pow() in the tone map (and so TAA) may
+# differ in the last bits.
 RTOL = 1e-3
 FLOOR = 1e-2
 
@@ -94,9 +94,7 @@ def test_stage_parity_over_frames(cuda, W, H):
         o.fitter(weights, mm, tmp, f)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(_np(g_mm), mm, err_msg=f"mins_maxs f={f}")
-        gw = _np(g_w)
-        exact = (gw == weights).mean()
-        assert exact > 0.99, f"weights bit-identical fraction {exact:.4f} f={f}"
+        np.testing.assert_array_equal(_np(g_w), weights, err_msg=f"weights f={f}")
 
         # --- weighted_sum with the oracle's weights
         g_out = torch.zeros(px * 3, dtype=torch.float32, device=cuda)

@@ -35,14 +35,18 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def test_oracle_reproduces_reference_pipeline_fixture():
-    g = np.load(GOLDEN / "ref_pipeline.npz")
+@pytest.mark.parametrize("fixture,use_half", [("ref_pipeline.npz", True), ("ref_pipeline_f32.npz", False)])
+def test_oracle_reproduces_reference_pipeline_fixture(fixture, use_half):
+    """binary16 tmp_data (the reference's default) and float32 tmp_data
+    (its USE_HALF_PRECISION_IN_TMP_DATA=0), on the same scene frames."""
+    inp = np.load(GOLDEN / "ref_pipeline.npz")
+    g = np.load(GOLDEN / fixture)
     frames = sum(1 for k in g.files if k.endswith("_result"))
-    H, W = g["in0_albedo"].shape[:2]
+    H, W = inp["in0_albedo"].shape[:2]
     lim = g["limits"]
-    pipe = OraclePipeline(Oracle(W, H, float(lim[0]), float(lim[1])))
+    pipe = OraclePipeline(Oracle(W, H, float(lim[0]), float(lim[1]), use_half=use_half))
     for f in range(frames):
-        res = pipe.step(*(g[f"in{f}_{k}"] for k in ("albedo", "normals", "positions", "noisy", "matrix", "offset")))
+        res = pipe.step(*(inp[f"in{f}_{k}"] for k in ("albedo", "normals", "positions", "noisy", "matrix", "offset")))
         c = f & 1
         same(res, g[f"out{f}_result"], f"result {f}")
         same(pipe.tone_mapped, g[f"out{f}_tone_mapped"], f"tone mapped {f}")
@@ -52,7 +56,8 @@ def test_oracle_reproduces_reference_pipeline_fixture():
         same(pipe.spp[c], g[f"out{f}_spp"], f"spp {f}")
         same(pipe.prev_pix, g[f"out{f}_prev_pix"], f"prev_frame_pixel {f}")
         same(pipe.noisy[c], g[f"out{f}_noisy_acc"], f"accumulated noisy {f}")
-        assert sha(pipe.tmp_after_accumulate.view(np.uint16)) == str(g[f"sha{f}_tmp"]), f"tmp_data {f}"
+        tmp_bits = pipe.tmp_after_accumulate.view(np.uint16 if use_half else np.uint32)
+        assert sha(tmp_bits) == str(g[f"sha{f}_tmp"]), f"tmp_data {f}"
         assert sha(pipe.filtered) == str(g[f"sha{f}_filtered"]), f"filtered {f}"
         assert sha(pipe.acc[c]) == str(g[f"sha{f}_acc"]), f"accumulated filtered {f}"
 
