@@ -38,7 +38,7 @@ def device_array(ptr, shape, dtype):
 
 
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
-@pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8)])
+@pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8), (197, 131, 5)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     import torch
     sc = B.Scene(21, W, H, 12)
