@@ -286,7 +286,9 @@ __device__ __forceinline__ void load_column(const Tile<HALF>& t, int k, int fb, 
 // One Householder column (bmfr.cl:549-655) on tile column 0; later columns
 // are tile columns 1..V.  NOISE: the first column, whose dot products read
 // features 1..9 with noise added (bmfr.cl:625-627).
-template <bool HALF, bool NOISE>
+// VS: column slots the loops visit (a compile-time bound >= the V later
+// columns): the late columns take a shorter instance.
+template <bool HALF, bool NOISE, int VS = 12>
 __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const float* __restrict__ noise,
                                           NoiseConst nc, FitterSmem& sm) {
     const int V = kBuffers - 1 - col;
@@ -319,9 +321,9 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
 
     // Dot products with the later columns (bmfr.cl:606-638), two columns at
     // a time in packed lanes; each lane keeps the reference's order.
-    float d[12];
+    float d[VS];
 #pragma unroll
-    for (int i = 0; i < 12; i += 2) {
+    for (int i = 0; i < VS; i += 2) {
         d[i] = d[i + 1] = 0.0f;
         if (i < V) {
             float2 a01, a23, b01, b23;
@@ -335,7 +337,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             d[i + 1] = s.y;
         }
     }
-    block_reduce<12, 0, 0>(d, V, V, sm);
+    block_reduce<VS, 0, 0>(d, V, V, sm);
 
     // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
     // Quotients take Markstein's correction when every operand is in range:
@@ -353,7 +355,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     }
     const float2 ny = dup2(-y), b2 = dup2(uls);
 #pragma unroll
-    for (int i = 0; i < 12; ++i) {
+    for (int i = 0; i < VS; ++i) {
         if (i < V) {
             const float dot = sm.out[i];
             const float ad = fabsf(dot);
@@ -830,7 +832,9 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
         }
         qr_column<HALF, true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1
-        for (int col = 1; col < kFeatures; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);
+        for (int col = 1; col < 6; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);        // 11..7 later columns
+#pragma unroll 1
+        for (int col = 6; col < kFeatures; ++col) qr_column<HALF, false, 6>(t, col, id, noise, nc, sm);   // 6..3
     }
 
     // After ten shifts the colour columns are tile columns 0..2: rows 0..9
