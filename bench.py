@@ -86,7 +86,7 @@ NCU_TRAFFIC_720P = {"fitter": 26.31e6, "accumulate_noisy_data": 66.8e6, "taa": 2
 # Warp instructions per launch at 1280x720 (smsp__inst_executed.sum of the
 # same captures): the numerator of the issue-rate roofline of a kernel that
 # is bound by instruction issue rather than by HBM.
-NCU_WARP_INST_720P = {"fitter": 63.5e6, "accumulate_noisy_data": 17.8e6, "taa": 11.0e6,
+NCU_WARP_INST_720P = {"fitter": 61.8e6, "accumulate_noisy_data": 17.8e6, "taa": 11.0e6,
                       "weighted_sum+accumulate_filtered_data": 12.4e6}
 SMS, SCHEDULERS_PER_SM = 148, 4
 
@@ -1072,7 +1072,7 @@ def main():
                 "frac": achieved / hbm_peak, "peak_source": peak_kind, "bytes_per_launch": sb[dominant],
                 "traffic": NCU_TRAFFIC_720P.get(dominant)}
     if dominant == "fitter":
-        roofline["note"] = ("the fitter is bound by instruction issue (ncu: 60 % issue active, 8.1 k instructions "
+        roofline["note"] = ("the fitter is bound by instruction issue (ncu: 60 % issue active, 7.85 k instructions "
                             "per thread per block), not by HBM or tensor cores; stages_gbs shows the HBM-bound stages")
     clk = clocks.summary()
     sm_mhz = clk.get("sm_mhz") or 1965.0
