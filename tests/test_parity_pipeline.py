@@ -38,7 +38,9 @@ def device_array(ptr, shape, dtype):
 
 
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
-@pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8), (197, 131, 5)])
+# 1280x720: 984 blocks, more than the persistent fitter's CTAs, so each CTA
+# fits several blocks through both tile buffers and both barrier phases.
+@pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8), (197, 131, 5), (1280, 720, 3)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     import torch
     sc = B.Scene(21, W, H, 12)
