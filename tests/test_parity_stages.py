@@ -43,7 +43,8 @@ def assert_close(got, want, what, rtol=RTOL, floor=FLOOR):
                            f"{np.nanmax(np.where(bad, err / np.maximum(np.abs(want), floor), 0)):.3e}")
 
 
-SIZES = [(64, 64), (100, 70), (256, 256)]
+# 1280x720: 984 blocks, more than the persistent fitter's CTAs.
+SIZES = [(64, 64), (100, 70), (256, 256), (1280, 720)]
 
 
 @pytest.mark.parametrize("W,H", SIZES)
