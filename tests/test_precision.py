@@ -45,10 +45,12 @@ def test_fp64_fitter_matches_oracle(cuda):
     plan.close()
 
 
+# 1280x720: more blocks than the persistent fitter's CTAs (each CTA fits
+# several blocks through both tile buffers).
+@pytest.mark.parametrize("W,H", [(256, 192), (1280, 720)])
 @pytest.mark.parametrize("qr", [B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
-def test_fp32_qr_weights_against_fp64(cuda, qr):
+def test_fp32_qr_weights_against_fp64(cuda, qr, W, H):
     import torch
-    W, H = 256, 192
     sc = B.Scene(17, W, H, 24)
     o = Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared)
     pipe = OraclePipeline(o)
