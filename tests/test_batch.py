@@ -117,6 +117,30 @@ def test_staged_step_with_more_streams_than_workers(cuda):
     batch.close()
 
 
+@pytest.mark.parametrize("qr", [B.QR_REFERENCE, B.QR_CHOLESKY2])
+def test_fused_step_queue_longer_than_the_grid(cuda, qr):
+    """Two 640x360 streams: 572 blocks in the fused step's queue, more than
+    its persistent CTAs, so CTAs take several blocks each; every result
+    equals its plan's bit for bit."""
+    import torch
+    kw = dict(fp32_qr=qr, half_history=1) if qr != B.QR_REFERENCE else {}
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, **kw)
+    streams = [Stream(40 + k, 640, 360, params, cuda) for k in range(2)]
+    batch = B.Batch(params)
+    slots = [batch.add_stream(s.w, s.h) for s in streams]
+    for f in range(3):
+        io = [s.io(f) for s in streams]
+        mats = np.concatenate([s.sc.prev_camera(f) for s in streams])
+        offs = np.concatenate([s.sc.pixel_offset(f) for s in streams])
+        batch.step(slots, mats, offs, io=io)
+        for k, s in enumerate(streams):
+            want = s.plan_step(f).cpu().numpy().reshape(s.h, s.w, 3)
+            np.testing.assert_array_equal(_device_result(batch.result_ptr(slots[k]), s.w, s.h), want,
+                                          err_msg=f"stream {k} frame {f}")
+    torch.cuda.synchronize()
+    batch.close()
+
+
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_FUSED, B.PIPELINE_STAGED])
 def test_batch_autotune_and_budget(cuda, pipeline):
     import torch
