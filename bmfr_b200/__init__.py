@@ -458,6 +458,10 @@ class Batch:
         check(lib.bmfr_batch_set_tuning(self.handle, C.byref(t)), "bmfr_batch_set_tuning")
 
     def autotune(self, slots, matrices, offsets, io=None, steps=3, stream=None):
+        """Times candidate tunings of the fused step on real steps of these
+        streams (advancing their histories) and keeps the fastest; the
+        staged step has nothing to tune and is only timed.  Returns
+        (tuning, mean ms per step)."""
         n, sl, iop, keep, mp, op = self._args(slots, io, matrices, offsets)
         t = BatchTuning()
         ms = C.c_float()
