@@ -238,7 +238,7 @@ def run_reference(args, world, rank):
               f"OpenMP over {cores} threads; {warm} warm-up frames")
     line = {
         "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
-        "steps": n, "steps_requested": args.steps, "warmup": warm, "warmup_requested": args.warmup,
+        "steps": n, "steps_requested": args.steps, "warmup": warm, "warmup_requested": args.warmup_requested,
         "ms_per_step": 1e3 * dt / n,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "BMFR plain pipeline 1280x720, 12-sphere procedural scene", "width": WIDTH,
@@ -978,7 +978,8 @@ def main():
     ap.add_argument("--seconds", type=float, default=10.0, help="served form: length of the arrival trace")
     ap.add_argument("--dump-pfm", default="", help="precision form: write the last frame's images (PFM) here")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
+    args.warmup_requested = args.warmup
+    args.warmup = max(args.warmup, 3)   # at least three untimed steps
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
