@@ -84,6 +84,18 @@ __device__ __forceinline__ int mirror(int i, int n) {
 
 // convert_int_rtn with defined results: NaN and magnitudes beyond 2^30 map to
 // +-2^30, outside every image.
+// Programmatic dependent launch.  The pipeline's kernels are launched with
+// programmatic stream serialization (launch_chained), so a kernel's launch
+// is processed while the kernel before it in the stream drains; before it
+// touches memory it waits here for that kernel's completion and memory
+// flush, which keeps exactly the ordering of a plain stream.  Dependents
+// are released implicitly as CTAs exit (no early trigger: released early,
+// waiting CTAs would take the SM slots that multi-wave grids still need).
+// Without the launch attribute this is a no-op.
+__device__ __forceinline__ void await_previous_kernel() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ int floor_to_int(float v) {
     if (!(v == v)) return -(1 << 30);
     const float f = floorf(v);

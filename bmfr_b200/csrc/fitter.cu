@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
     k_fitter(int nblocks, int frame, NoiseConst nc, const void* __restrict__ tmp, const __grid_constant__ CUtensorMap tmap,
              float* __restrict__ weights, float* __restrict__ mins_maxs, const float* __restrict__ noise_g,
              int* __restrict__ status) {
+    await_previous_kernel();
     using Shared = FitterShared<HALF_TMP, NOISE_GLOBAL>;
     using TmpT = typename Shared::TmpT;
     constexpr int kStages = Shared::kStages;
@@ -138,13 +139,13 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
 
 // The frame's noise table in global memory (kNoiseTableFloats floats).
 __global__ void __launch_bounds__(256) k_noise_table(int frame, float* __restrict__ table) {
+    await_previous_kernel();
     const int e = blockIdx.x * kLocal + threadIdx.x;
     if (e < kNoiseTableFloats) table[e] = noise_table_value(e, frame);
 }
 
 cudaError_t launch_noise_table(int frame, float* table, cudaStream_t s) {
-    k_noise_table<<<kNoiseTableFloats / kLocal, kLocal, 0, s>>>(frame, table);
-    return cudaGetLastError();
+    return launch_chained(k_noise_table, dim3(kNoiseTableFloats / kLocal), dim3(kLocal), 0, s, frame, table);
 }
 
 // A barrier that no copy or thread ever completes: thread 0's bounded wait
@@ -221,8 +222,8 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
         e = encode_tmp_map(tmp, nblocks, &map);
         if (e != cudaSuccess) return e;
     }
-    kern<<<grid, kLocal, smem, s>>>(nblocks, frame, nc, tmp, map, weights, mins_maxs, noise, status);
-    return cudaGetLastError();
+    return launch_chained(kern, dim3(grid), dim3(kLocal), smem, s, nblocks, frame, nc, tmp, map, weights,
+                          mins_maxs, noise, status);
 }
 
 cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,

@@ -3,10 +3,32 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <utility>
 
 #include "common.cuh"
 
 namespace bmfr {
+
+// Launches `kern` with programmatic stream serialization: its launch is
+// processed while the previous kernel in the stream drains, and the kernel
+// begins with await_previous_kernel() (common.cuh), so the stream's ordering
+// is unchanged.  Measured on a 1280x720 frame of the plan pipeline: 164.8
+// against 174.7 us with plain launches.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // noisy_out/prev_noisy: the accumulated-colour history, float or (with
 // half_history) binary16; noisy_in == noisy_out runs the in-place form.

@@ -29,6 +29,7 @@ __global__ void __launch_bounds__(256) k_accumulate_noisy(
     const float* __restrict__ cur_p, const float* __restrict__ prev_p,
     const float* noisy_in, HistT* noisy_out, const HistT* __restrict__ prev_noisy,
     const uint8_t* __restrict__ prev_spp, uint8_t* __restrict__ cur_spp, void* __restrict__ tmp) {
+    await_previous_kernel();
     const int gx = blockIdx.x * 32 + threadIdx.x;
     const int gy = blockIdx.y * 8 + threadIdx.y;
     if constexpr (MODE == 0) {
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(256) k_weighted_sum_accumulate(
     const float* __restrict__ albedo, float* __restrict__ tone_mapped,
     const uint8_t* __restrict__ cur_spp, const HistT* __restrict__ acc_prev,
     HistT* __restrict__ acc_cur) {
+    await_previous_kernel();
     const int px = blockIdx.x * 32 + threadIdx.x, py = blockIdx.y * 8 + threadIdx.y;
     if (px >= g.W || py >= g.H) return;
     wsacc_px<HistT>(g, frame, second_alpha, px, py, weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept,
@@ -124,6 +126,7 @@ __global__ void __launch_bounds__(128) k_taa(Geometry g, int frame, float taa_al
                                              HistT* __restrict__ result,
                                              const HistT* __restrict__ prev_frame,
                                              float* __restrict__ result_f32) {
+    await_previous_kernel();
     taa_strip<kTaaRows, HistT>(g, frame, taa_alpha, blockIdx.x * 30, (blockIdx.y * 4 + (threadIdx.x >> 5)) * kTaaRows,
                                prev_pix, new_frame, prev_frame, result, result_f32);
 }
@@ -142,25 +145,23 @@ cudaError_t launch_accumulate_noisy(const Geometry& g, const AccumArgs& a, float
                                     const float* prev_p, const float* noisy_in, void* noisy_out,
                                     const void* prev_noisy, bool half_history, const uint8_t* prev_spp,
                                     uint8_t* cur_spp, void* tmp, cudaStream_t s) {
-    const dim3 block(32, 8);
-    if (half_history) {
-        k_accumulate_noisy<0, __half><<<margin_grid(g), block, 0, s>>>(
-            g, a, prev_pix, accept, cur_n, prev_n, cur_p, prev_p, noisy_in, (__half*)noisy_out,
-            (const __half*)prev_noisy, prev_spp, cur_spp, tmp);
-    } else if (noisy_in == noisy_out) {
+    const dim3 grid = margin_grid(g), block(32, 8);
+    if (half_history)
+        return launch_chained(k_accumulate_noisy<0, __half>, grid, block, 0, s, g, a, prev_pix, accept, cur_n,
+                              prev_n, cur_p, prev_p, noisy_in, (__half*)noisy_out, (const __half*)prev_noisy,
+                              prev_spp, cur_spp, tmp);
+    if (noisy_in == noisy_out) {
         float* io = (float*)noisy_out;
-        k_accumulate_noisy<1, float><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
-                                                                      prev_p, noisy_in, io, (const float*)prev_noisy,
-                                                                      prev_spp, cur_spp, tmp);
-        k_accumulate_noisy<2, float><<<margin_grid(g), block, 0, s>>>(g, a, prev_pix, accept, cur_n, prev_n, cur_p,
-                                                                      prev_p, noisy_in, io, (const float*)prev_noisy,
-                                                                      prev_spp, cur_spp, tmp);
-    } else {
-        k_accumulate_noisy<0, float><<<margin_grid(g), block, 0, s>>>(
-            g, a, prev_pix, accept, cur_n, prev_n, cur_p, prev_p, noisy_in, (float*)noisy_out,
-            (const float*)prev_noisy, prev_spp, cur_spp, tmp);
+        const cudaError_t e = launch_chained(k_accumulate_noisy<1, float>, grid, block, 0, s, g, a, prev_pix, accept,
+                                             cur_n, prev_n, cur_p, prev_p, noisy_in, io, (const float*)prev_noisy,
+                                             prev_spp, cur_spp, tmp);
+        if (e != cudaSuccess) return e;
+        return launch_chained(k_accumulate_noisy<2, float>, grid, block, 0, s, g, a, prev_pix, accept, cur_n, prev_n,
+                              cur_p, prev_p, noisy_in, io, (const float*)prev_noisy, prev_spp, cur_spp, tmp);
     }
-    return cudaGetLastError();
+    return launch_chained(k_accumulate_noisy<0, float>, grid, block, 0, s, g, a, prev_pix, accept, cur_n, prev_n,
+                          cur_p, prev_p, noisy_in, (float*)noisy_out, (const float*)prev_noisy, prev_spp, cur_spp,
+                          tmp);
 }
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,
@@ -186,28 +187,22 @@ cudaError_t launch_weighted_sum_accumulate(const Geometry& g, int frame, float s
                                            const uint8_t* cur_spp, const void* acc_prev, void* acc_cur,
                                            bool half_history, cudaStream_t s) {
     if (half_history)
-        k_weighted_sum_accumulate<__half><<<image_grid(g), dim3(32, 8), 0, s>>>(
-            g, frame, second_alpha, weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept, albedo,
-            tone_mapped, cur_spp, (const __half*)acc_prev, (__half*)acc_cur);
-    else
-        k_weighted_sum_accumulate<float><<<image_grid(g), dim3(32, 8), 0, s>>>(
-            g, frame, second_alpha, weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept, albedo,
-            tone_mapped, cur_spp, (const float*)acc_prev, (float*)acc_cur);
-    return cudaGetLastError();
+        return launch_chained(k_weighted_sum_accumulate<__half>, image_grid(g), dim3(32, 8), 0, s, g, frame,
+                              second_alpha, weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept, albedo,
+                              tone_mapped, cur_spp, (const __half*)acc_prev, (__half*)acc_cur);
+    return launch_chained(k_weighted_sum_accumulate<float>, image_grid(g), dim3(32, 8), 0, s, g, frame, second_alpha,
+                          weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept, albedo, tone_mapped, cur_spp,
+                          (const float*)acc_prev, (float*)acc_cur);
 }
 
 cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const float2* prev_pix,
                        const float* new_frame, void* result, const void* prev_frame, float* result_f32,
                        bool half_history, cudaStream_t s) {
     if (half_history)
-        k_taa<__half><<<taa_grid(g), 128, 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
-                                                           (__half*)result, (const __half*)prev_frame,
-                                                           result_f32);
-    else
-        k_taa<float><<<taa_grid(g), 128, 0, s>>>(g, frame, taa_alpha, prev_pix, new_frame,
-                                                          (float*)result, (const float*)prev_frame,
-                                                          result_f32);
-    return cudaGetLastError();
+        return launch_chained(k_taa<__half>, taa_grid(g), dim3(128), 0, s, g, frame, taa_alpha, prev_pix, new_frame,
+                              (__half*)result, (const __half*)prev_frame, result_f32);
+    return launch_chained(k_taa<float>, taa_grid(g), dim3(128), 0, s, g, frame, taa_alpha, prev_pix, new_frame,
+                          (float*)result, (const float*)prev_frame, result_f32);
 }
 
 }  // namespace bmfr
