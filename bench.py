@@ -8,19 +8,29 @@ backwards.  One step = one denoised frame.
 
 Our arm prints one JSON line with
   value      frames/s of the plan pipeline (staged by default), inputs
-             resident in HBM (all ranks),
+             resident in HBM (all ranks); the K-step loop repeats until at
+             least 0.5 s have passed and its median gives the step time,
   e2e        frames/s through the C ABI from pinned host buffers, with the
              four input uploads and the result download inside the timed region,
   stages     ms per stage (the reference's per-kernel profile, bmfr.cpp:488-517),
-  roofline   the dominant kernel's achieved HBM bandwidth against the measured
-             copy bandwidth, and (`issue`) its warp-instruction rate against
-             the SMs' issue rate, the bound of an issue-bound kernel,
+  roofline   the dominant kernel against its bound: the fitter's warp-
+             instruction rate against the SMs' issue rate (it is issue-bound),
+             with its HBM figures beside it; an HBM-bound kernel's bandwidth
+             against the measured copy bandwidth,
+  batched    the multi-stream half of the metric: 24 streams of uneven size
+             per step, frames/s, step latency p50/p99, and the ratios to the
+             plain path and to plans of the same arithmetic,
+  served     64 Poisson render streams through the request server: frames/s
+             and frame latency p50/p99, beside the plain path on the same
+             trace, and the capacity of both,
   cpu_baseline  the reference's own OpenCL kernels compiled for the CPU
              (oracle/_ref) on a bounded sample of frames on this host's cores,
              with the oracle port's figure beside it.
 --impl reference times the reference's kernels alone (the port where they
-are not built).  Under torchrun every rank denoises its own stream
-(replicas, no collective on the data path); rank 0 prints.
+are not built).  --gpus N starts N ranks, one process per GPU, unless a
+launcher already did (a rank count other than N is an error); every rank
+denoises its own streams (replicas, no collective on the data path) and
+rank 0 prints.
 """
 from __future__ import annotations
 
@@ -38,7 +48,12 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from bmfr_b200.replicas import max_over_ranks  # noqa: E402
+
+def max_over_ranks(value, device=None):
+    """The slowest rank's value (bmfr_b200.replicas; imported here so that the
+    reference arm maps no pipeline code)."""
+    from bmfr_b200.replicas import max_over_ranks as m
+    return m(value, device=device)
 
 WIDTH, HEIGHT, FRAMES, SPHERES, SEED = 1280, 720, 60, 12, 20240601
 METRIC = "720p frames/s, full BMFR pipeline (accumulate, fitter, weighted sum, filtered accumulation, TAA)"
@@ -89,6 +104,41 @@ NCU_TRAFFIC_720P = {"fitter": 26.31e6, "accumulate_noisy_data": 66.8e6, "taa": 2
 NCU_WARP_INST_720P = {"fitter": 61.8e6, "accumulate_noisy_data": 17.8e6, "taa": 11.0e6,
                       "weighted_sum+accumulate_filtered_data": 12.4e6}
 SMS, SCHEDULERS_PER_SM = 148, 4
+# Kernels bound by instruction issue rather than by HBM or tensor cores.
+ISSUE_BOUND = {"fitter": "the fitter is a sequence of small dependent reductions and rank-one updates kept "
+                         "bit-identical to the reference (no FMA contraction, correctly rounded quotients, binary16 "
+                         "rounding at every store): bound by instruction issue, not by HBM (it reads its 26 MB "
+                         "once) or tensor cores; stages_gbs shows the HBM-bound stages"}
+
+
+MIN_TIMED_SECONDS = 0.5   # each timed region repeats its K-step loop at least this long
+
+
+def timed_loops(run_steps, stream, dev, min_seconds=MIN_TIMED_SECONDS, max_loops=2000):
+    """Times `run_steps(loop)` (one loop = K steps launched on `stream`) with
+    CUDA events on `stream`, repeating the loop until `min_seconds` of device
+    time have passed, so that the clock sampler sees the run.  The first loop
+    sets the count, the largest over ranks, so every rank takes the same
+    collective steps.  Returns the device milliseconds of every loop."""
+    import torch
+    evs = []
+
+    def one(loop):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_steps(loop)
+        e1.record(stream)
+        evs.append((e0, e1))
+
+    one(0)
+    evs[0][1].synchronize()
+    first = evs[0][0].elapsed_time(evs[0][1])
+    loops = int(min(max_loops, max(1, -(-min_seconds * 1e3 // max(first, 1e-3)))))
+    loops = int(max_over_ranks(float(loops), device=dev))
+    for loop in range(1, loops):
+        one(loop)
+    evs[-1][1].synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
 
 
 def frame_order(i, n):
@@ -142,6 +192,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def launch_command(gpus, argv, port=None):
+    """The command that runs this benchmark as `gpus` ranks on this node, one
+    process per GPU, rendezvous on 127.0.0.1."""
+    if port is None:
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *argv]
+
+
+def check_world(world, gpus):
+    """A run whose rank count differs from --gpus is an error, not a silent
+    one-GPU measurement."""
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started {world} rank(s)")
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -150,8 +219,8 @@ def dist_setup():
 
 
 def render_frames(seed, w, h, n):
-    import bmfr_b200 as B
-    sc = B.Scene(seed, w, h, SPHERES)
+    from bmfr_scene import Scene   # the input source alone: no pipeline library
+    sc = Scene(seed, w, h, SPHERES)
     frames = [sc.render(f) for f in range(n)]
     return sc, frames
 
@@ -271,12 +340,15 @@ def batch_scenes(rank):
             for k, (w, h) in enumerate(BATCH_STREAMS)]
 
 
-def run_batched(args, world, rank, local, dev, barrier, pg):
+def measure_batched(args, world, rank, local, dev, barrier, steps, warmup):
     """Batched form: 24 streams of uneven size, one step per frame of every
     stream (staged: each stream's plan kernels on eight worker CUDA streams;
     fused: one graph-captured launch over all streams' blocks), binary16
-    histories and FP32 QR; next to the plain per-frame path on the same
-    streams."""
+    histories and FP32 QR (CholeskyQR2).  Beside it, the same streams one
+    frame at a time through (a) the plain path (reference arithmetic, float
+    histories: the north star's baseline) and (b) plans with the batch's own
+    arithmetic and histories (the gain of batching alone).  Returns the
+    measurement as a dict."""
     import torch
     import bmfr_b200 as B
     scenes = batch_scenes(rank)
@@ -314,69 +386,98 @@ def run_batched(args, world, rank, local, dev, barrier, pg):
     tuning, tuned_ms = batch.autotune(slots, m0, o0, io=io0, steps=2, stream=stream)
     for sl in slots:
         batch.reset_stream(sl)
-    for i in range(args.warmup):
-        io, m, o = step_args(i)
+    # Step arguments prepared up front: the timed loop only launches.
+    prepared = [step_args(i) for i in range(2 * (nfr - 1))]
+    for i in range(warmup):
+        io, m, o = prepared[i % len(prepared)]
         batch.step(slots, m, o, io=io, stream=stream)
     stream.synchronize()
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        e0.record(stream)
-        for i in range(args.warmup, args.warmup + args.steps):
-            io, m, o = step_args(i)
+    step_events = []
+
+    def k_steps(loop):
+        for i in range(steps):
+            io, m, o = prepared[(warmup + loop * steps + i) % len(prepared)]
             batch.step(slots, m, o, io=io, stream=stream)
-        e1.record(stream)
-        e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, device=dev)   # the slowest rank
-    value = world * n * args.steps / (ms / 1e3)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+            step_events.append(ev)
+
+    with ClockSampler(local) as clocks:
+        loop_ms = timed_loops(k_steps, stream, dev)
+    stream.synchronize()
+    # Device time of each step: between the events that close it and the
+    # step before it (the first step of each loop is left out).
+    per_step = [step_events[j - 1].elapsed_time(step_events[j]) for j in range(1, len(step_events))
+                if j % steps != 0]
+    ms = max_over_ranks(statistics.median(loop_ms), device=dev)   # the slowest rank
+    value = world * n * steps / (ms / 1e3)
     batch.close()
 
-    # The plain path (reference arithmetic, float histories, staged pipeline)
-    # on the same streams, one frame at a time.
-    plans = [B.Plan(sc.width, sc.height, position_limit_squared=sc.position_limit_squared,
-                    normal_limit_squared=sc.normal_limit_squared) for sc in scenes]
-    plain_steps = min(args.steps, 10)
+    def plans_in_turn(plan_kw, rounds):
+        """The same streams one frame at a time through their own plans."""
+        plans = [B.Plan(sc.width, sc.height, position_limit_squared=sc.position_limit_squared,
+                        normal_limit_squared=sc.normal_limit_squared, **plan_kw) for sc in scenes]
 
-    def plain_step(i):
-        f = frame_order(i, nfr)
-        pf = frame_order(i - 1, nfr) if i > 0 else f
-        for k, (sc, pl) in enumerate(zip(scenes, plans)):
-            d, p = frames[k][f], frames[k][pf]
-            pl.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"], p["positions"],
-                                sc.camera(pf), sc.pixel_offset(f), stream=stream)
+        def one_round(i):
+            f = frame_order(i, nfr)
+            pf = frame_order(i - 1, nfr) if i > 0 else f
+            for k, (sc, pl) in enumerate(zip(scenes, plans)):
+                d, p = frames[k][f], frames[k][pf]
+                pl.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"],
+                                    p["positions"], sc.camera(pf), sc.pixel_offset(f), stream=stream)
 
-    for i in range(3):
-        plain_step(i)
-    stream.synchronize()
-    e0.record(stream)
-    for i in range(3, 3 + plain_steps):
-        plain_step(i)
-    e1.record(stream)
-    e1.synchronize()
-    plain_ms = e0.elapsed_time(e1)
-    plain_value = n * plain_steps / (plain_ms / 1e3)
-    for pl in plans:
-        pl.close()
+        for i in range(3):
+            one_round(i)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(3, 3 + rounds):
+            one_round(i)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1)
+        for pl in plans:
+            pl.close()
+        return n * rounds / (t / 1e3), t / rounds
+
+    rounds = max(3, min(steps, 10))
+    plain_value, plain_round_ms = plans_in_turn({}, rounds)
+    prec_value, prec_round_ms = plans_in_turn(dict(fp32_qr=1, half_history=1, pipeline=pipeline), rounds)
     pixels = sum(w * h for w, h in BATCH_STREAMS)
+    return {
+        "metric": "multi-stream frames/s (24 streams: 8x640x360, 8x1280x720, 6x1920x1080, 2x3840x2160)",
+        "value": value, "unit": "frames/s", "steps": steps, "timed_loops": len(loop_ms),
+        "ms_per_step": ms / steps,
+        "step_latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99)),
+                            "how": "device time of each step (every stream's frame is done when its step ends)"},
+        "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered, 30 frames per stream)",
+        "config": {"workload": "batched form, 24 streams", "streams": len(BATCH_STREAMS), "pipeline": args.pipeline,
+                   "qr": "CholeskyQR2 (FP32)", "pixels_per_step": pixels, "frames": nfr, "tuning": {
+                       "block_ctas_per_sm": tuning.block_ctas_per_sm, "taa_tile": [tuning.taa_tile_w, tuning.taa_tile_h],
+                       "staging_depth": tuning.staging_depth}, "tuned_ms_per_step": tuned_ms},
+        "plain_path": {"value": plain_value, "unit": "frames/s", "ms_per_round": plain_round_ms,
+                       "how": "one plan per stream, staged pipeline, reference arithmetic, float histories, "
+                              "frames in turn"},
+        "same_arithmetic_plans": {"value": prec_value, "unit": "frames/s", "ms_per_round": prec_round_ms,
+                                  "how": "one plan per stream with the batch's parameters (CholeskyQR2, binary16 "
+                                         "histories, same pipeline), frames in turn"},
+        "speedup_vs_plain": value / plain_value / world,
+        "speedup_vs_same_arithmetic_plans": value / prec_value / world,
+        "clocks": clocks.summary(),
+        # per step: noise table, block kernel, TAA (fused); per stream noise
+        # table, accumulation, fitter, weighted sum + filtered accumulation, TAA (staged)
+        "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 5 * n) * steps * len(loop_ms),
+    }
+
+
+def run_batched(args, world, rank, local, dev, barrier, pg):
+    """--form batched: the batched measurement as its own JSON line."""
+    r = measure_batched(args, world, rank, local, dev, barrier, args.steps, args.warmup)
     if rank == 0:
-        print(json.dumps({
-            "form": "batched", "metric": "multi-stream frames/s (24 streams: 8x640x360, 8x1280x720, 6x1920x1080, 2x3840x2160)",
-            "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered, 30 frames per stream)",
-            "config": {"workload": "batched form, 24 streams", "streams": len(BATCH_STREAMS), "pipeline": args.pipeline,
-                       "pixels_per_step": pixels, "frames": nfr, "tuning": {
-                           "block_ctas_per_sm": tuning.block_ctas_per_sm, "taa_tile": [tuning.taa_tile_w, tuning.taa_tile_h],
-                           "staging_depth": tuning.staging_depth}, "tuned_ms_per_step": tuned_ms},
-            "plain_path": {"value": plain_value, "unit": "frames/s", "ms_per_round": plain_ms / plain_steps,
-                           "how": "one plan per stream, staged pipeline, reference arithmetic, frames in turn"},
-            "speedup_vs_plain": value / plain_value / world,
-            # per step: noise table, block kernel, TAA (fused); per stream noise
-            # table, accumulation, fitter, weighted sum + filtered accumulation, TAA (staged)
-            "clocks": clocks.summary(),
-            "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 5 * n) * args.steps,
-        }), flush=True)
+        r.update({"form": "batched", "n_gpus": world, "warmup": args.warmup, "higher_is_better": True,
+                  "scaling": "weak", "vs_baseline": None})
+        print(json.dumps(r), flush=True)
 
 
 SERVED_SEATS = 64
@@ -426,11 +527,12 @@ def drive_trace(events, t0, on_event):
         on_event(ev)
 
 
-def run_served(args, world, rank, local, dev, barrier, pg):
+def measure_served(args, world, rank, local, dev, barrier, seconds):
     """Served form: 64 render streams with Poisson frame requests at 30/60 Hz,
     joining and leaving, histories resident in HBM, admission against a
     120 GB budget; the request server (continuous batching) next to the
-    plain per-frame path fed the same trace."""
+    plain per-frame path fed the same trace, and the capacity of both (every
+    stream always ready).  Returns the measurement as a dict."""
     import queue
     import threading
     from concurrent.futures import ThreadPoolExecutor
@@ -461,7 +563,7 @@ def run_served(args, world, rank, local, dev, barrier, pg):
                               fp32_qr=1, half_history=1,
                               position_limit_squared=pools[0]["sc"].position_limit_squared,
                               normal_limit_squared=pools[0]["sc"].normal_limit_squared)
-    seconds = float(args.seconds)
+    seconds = float(seconds)
     warm_s = min(1.0, seconds / 4)
     events, streams = served_trace(SEED + 4242 + rank, seconds)
     n_req = sum(1 for e in events if e[1] == 1 and e[0] >= warm_s)
@@ -501,26 +603,34 @@ def run_served(args, world, rank, local, dev, barrier, pg):
 
     plain_params = dict(position_limit_squared=params.position_limit_squared,
                         normal_limit_squared=params.normal_limit_squared)
-    cap_plans = [B.Plan(pools[st["cls"]]["w"], pools[st["cls"]]["h"], **plain_params) for st in cap_streams]
 
-    def plain_round(i):
-        for st, pl in zip(cap_streams, cap_plans):
-            _, m, o, d, p = pools[st["cls"]]["tab"][(st["phase"] + i) % period]
-            pl.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"],
-                                p["positions"], m, o, stream=stream)
+    def capacity_of_plans(kw):
+        cap_plans = [B.Plan(pools[st["cls"]]["w"], pools[st["cls"]]["h"], **plain_params, **kw)
+                     for st in cap_streams]
 
-    for i in range(3):
-        plain_round(i)
-    plain_rounds = 5
-    e0.record(stream)
-    for i in range(3, 3 + plain_rounds):
-        plain_round(i)
-    e1.record(stream)
-    e1.synchronize()
-    cap_plain = len(cap_streams) * plain_rounds / (e0.elapsed_time(e1) / 1e3)
-    for pl in cap_plans:
-        pl.close()
-    torch.cuda.synchronize()
+        def plain_round(i):
+            for st, pl in zip(cap_streams, cap_plans):
+                _, m, o, d, p = pools[st["cls"]]["tab"][(st["phase"] + i) % period]
+                pl.denoise_frame_io(d["albedo"], d["normals"], d["positions"], d["noisy"], p["normals"],
+                                    p["positions"], m, o, stream=stream)
+
+        for i in range(3):
+            plain_round(i)
+        plain_rounds = 5
+        e0.record(stream)
+        for i in range(3, 3 + plain_rounds):
+            plain_round(i)
+        e1.record(stream)
+        e1.synchronize()
+        v = len(cap_streams) * plain_rounds / (e0.elapsed_time(e1) / 1e3)
+        for pl in cap_plans:
+            pl.close()
+        torch.cuda.synchronize()
+        return v
+
+    cap_plain = capacity_of_plans({})
+    cap_same = capacity_of_plans(dict(fp32_qr=params.fp32_qr, half_history=params.half_history,
+                                      pipeline=params.pipeline))
 
     # Peak stream memory and peak open streams per class over the trace:
     # both paths reserve them before the trace starts.
@@ -696,12 +806,10 @@ def run_served(args, world, rank, local, dev, barrier, pg):
             plain_by_second.setdefault(int(ta - t0p), []).append(1e3 * l)
     plain_fps = len(kept) / max(t_endp - (t0p + warm_s), 1e-9)
 
-    if rank == 0:
-        print(json.dumps({
-            "form": "served", "metric": "served form: aggregate frames/s with p50/p99 frame latency, 64 Poisson streams",
-            "value": world * served_fps, "unit": "frames/s", "n_gpus": world, "steps": int(st["steps"]),
-            "warmup": 0, "ms_per_step": 1e3 * st["busy_seconds"] / max(st["steps"], 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    return {
+            "metric": "served form: aggregate frames/s with p50/p99 frame latency, 64 Poisson streams",
+            "value": world * served_fps, "unit": "frames/s", "steps": int(st["steps"]),
+            "ms_per_step": 1e3 * st["busy_seconds"] / max(st["steps"], 1),
             "dtype": "f32 math, f16 histories", "data": "synthetic (device-rendered frame pools)",
             "config": {"workload": "served form, 64 Poisson streams", "seats": SERVED_SEATS, "pipeline": args.pipeline,
                        "mix": [[w, h, p] for (w, h), p in SERVED_MIX], "rates_hz": [30, 60],
@@ -730,6 +838,7 @@ def run_served(args, world, rank, local, dev, barrier, pg):
                            "how": "one staged plan per stream (reference arithmetic, float histories), "
                                   "requests in arrival order on one CUDA stream, plans reused across streams"},
             "capacity": {"batched": cap_batched, "plain": cap_plain, "ratio": cap_batched / cap_plain,
+                         "same_arithmetic_plans": cap_same, "ratio_vs_same_arithmetic": cap_batched / cap_same,
                          "unit": "frames/s", "streams": len(cap_streams),
                          "how": "every seat's first stream with a frame ready at every step; batched: one "
                                 "step per frame of all streams (staged: each stream's plan kernels on eight "
@@ -738,7 +847,16 @@ def run_served(args, world, rank, local, dev, barrier, pg):
             # per step: 5 kernels per listed stream (staged) or noise, block kernel, TAA (fused)
             "clocks": clocks.summary(),
             "gpu_launches": (5 * int(st.get("frames", 0)) if args.pipeline == "staged" else 3 * int(st["steps"])),
-        }), flush=True)
+        }
+
+
+def run_served(args, world, rank, local, dev, barrier, pg):
+    """--form served: the served measurement as its own JSON line."""
+    r = measure_served(args, world, rank, local, dev, barrier, args.seconds)
+    if rank == 0:
+        r.update({"form": "served", "n_gpus": world, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+                  "vs_baseline": None})
+        print(json.dumps(r), flush=True)
 
 
 PRECISION_W, PRECISION_H, PRECISION_FRAMES, PRECISION_SPHERES = 1920, 1080, 60, 24
@@ -977,10 +1095,20 @@ def main():
     ap.add_argument("--qr", type=int, default=0, help="probe form: fp32_qr of the plan (0, 1 or 2)")
     ap.add_argument("--seconds", type=float, default=10.0, help="served form: length of the arrival trace")
     ap.add_argument("--dump-pfm", default="", help="precision form: write the last frame's images (PFM) here")
+    ap.add_argument("--no-multistream", action="store_true",
+                    help="plain form: leave out the batched and served objects of the line")
+    ap.add_argument("--served-seconds", type=float, default=4.0,
+                    help="plain form: length of the served object's arrival trace")
     args = ap.parse_args()
     args.warmup_requested = args.warmup
     args.warmup = max(args.warmup, 3)   # at least three untimed steps
+    if args.gpus < 1:
+        ap.error("--gpus must be at least 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # One process per GPU: start N ranks of this same command.
+        sys.exit(subprocess.call(launch_command(args.gpus, sys.argv[1:])))
     world, rank, local = dist_setup()
+    check_world(world, args.gpus)
 
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -1038,17 +1166,19 @@ def main():
     stream.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # The K-step loop repeats until at least MIN_TIMED_SECONDS have passed;
+    # the loop's median time, the slowest rank's, gives the step time.
+    base0 = args.warmup
+
+    def k_steps(loop):
+        for i in range(args.steps):
+            step_resident(base0 + loop * args.steps + i)
+
     with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for i in range(args.warmup, args.warmup + args.steps):
-            step_resident(i)
-        ev1.record(stream)
-        ev1.synchronize()
+        loop_ms = timed_loops(k_steps, stream, dev)
     torch.cuda.synchronize()
     barrier()
-    elapsed_ms = ev0.elapsed_time(ev1)
-    elapsed_ms = max_over_ranks(elapsed_ms, device=dev)   # the slowest rank
+    elapsed_ms = max_over_ranks(statistics.median(loop_ms), device=dev)   # the slowest rank
     value = world * args.steps / (elapsed_ms / 1e3)
     # noise table, block kernel, taa (fused); noise table, accumulate, fitter,
     # weighted sum + filtered accumulation, taa (staged)
@@ -1057,7 +1187,7 @@ def main():
     # ---- per-stage profile (same workload, events between stages) ------------
     plan.enable_profiling(True)
     stage_ms = {}
-    base = args.warmup + args.steps
+    base = args.warmup + len(loop_ms) * args.steps
     nprof = min(args.steps, 60)
     for i in range(base, base + nprof):
         step_resident(i)
@@ -1069,21 +1199,28 @@ def main():
     dominant = max(stages, key=stages.get)
     hbm_peak, peak_kind = peaks()
     achieved = sb[dominant] / (stages[dominant] * 1e-3) / 1e9
-    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "peak_source": peak_kind, "bytes_per_launch": sb[dominant],
-                "traffic": NCU_TRAFFIC_720P.get(dominant)}
-    if dominant == "fitter":
-        roofline["note"] = ("the fitter is bound by instruction issue (ncu: 60 % issue active, 7.85 k instructions "
-                            "per thread per block), not by HBM or tensor cores; stages_gbs shows the HBM-bound stages")
+    hbm = {"achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+           "peak_source": peak_kind, "bytes_per_launch": sb[dominant], "traffic": NCU_TRAFFIC_720P.get(dominant)}
     clk = clocks.summary()
     sm_mhz = clk.get("sm_mhz") or 1965.0
     issue_peak = SMS * SCHEDULERS_PER_SM * sm_mhz * 1e6 / 1e9          # G warp-instructions/s
+    issue = None
     if dominant in NCU_WARP_INST_720P:
         got = NCU_WARP_INST_720P[dominant] / (stages[dominant] * 1e-3) / 1e9
-        roofline["issue"] = {"achieved": got, "peak": issue_peak, "unit": "G warp-instructions/s",
-                             "frac": got / issue_peak, "instructions_per_launch": NCU_WARP_INST_720P[dominant],
-                             "peak_source": f"{SMS} SMs x {SCHEDULERS_PER_SM} schedulers x 1 instruction/cycle at "
-                                            f"the sampled SM clock ({sm_mhz:.0f} MHz)"}
+        issue = {"achieved": got, "peak": issue_peak, "unit": "G warp-instructions/s",
+                 "frac": got / issue_peak, "instructions_per_launch": NCU_WARP_INST_720P[dominant],
+                 "peak_source": f"{SMS} SMs x {SCHEDULERS_PER_SM} schedulers x 1 instruction/cycle at "
+                                f"the sampled SM clock ({sm_mhz:.0f} MHz)"}
+    if dominant in ISSUE_BOUND and issue is not None:
+        # An issue-bound kernel: the issue rate leads, the HBM figures ride along.
+        roofline = {"kernel": dominant, "bound": "issue", **{k: issue[k] for k in ("achieved", "peak", "unit", "frac")},
+                    "peak_source": issue["peak_source"], "instructions_per_launch": issue["instructions_per_launch"],
+                    "traffic": NCU_TRAFFIC_720P.get(dominant), "hbm": hbm,
+                    "note": ISSUE_BOUND[dominant]}
+    else:
+        roofline = {"kernel": dominant, "bound": "hbm", **{k: hbm[k] for k in hbm}}
+        if issue is not None:
+            roofline["issue"] = issue
     stage_gbs = {k: sb[k] / (v * 1e-3) / 1e9 for k, v in stages.items() if v > 0}
     dropin = dropin_stage_ms(B, torch, dev, stream, plan.params, devf, mats, off, min(args.steps, 30))
 
@@ -1107,7 +1244,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = min(args.steps, 120)
+    e2e_steps = min(max(args.steps, 100), 300)   # ~0.1-0.3 s of PCIe-bound frames
     e0.record(up_stream)
     for i in range(args.warmup, args.warmup + e2e_steps):
         step_e2e(i)
@@ -1118,11 +1255,23 @@ def main():
     e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": "frames/s",
            "h2d_bytes_per_step": 4 * WIDTH * HEIGHT * 12, "d2h_bytes_per_step": WIDTH * HEIGHT * 12}
 
+    plan.close()
+    del devf
+    torch.cuda.synchronize()
+
+    # ---- the multi-stream half of the metric: batched and served forms -------
+    multi = {}
+    if not args.no_multistream:
+        mst = max(args.steps, 10)
+        multi["batched"] = measure_batched(args, world, rank, local, dev, barrier, mst, args.warmup)
+        torch.cuda.synchronize()
+        multi["served"] = measure_served(args, world, rank, local, dev, barrier, args.served_seconds)
+        torch.cuda.synchronize()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(frames, sc, ref_budget_s=15.0, port_budget_s=10.0)
 
-    plan.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -1136,8 +1285,11 @@ def main():
             "dropin_stages_ms": dropin,
             "dropin_stages_gbs": {k: sb[k] / (v * 1e-3) / 1e9 for k, v in dropin.items() if v > 0},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clk, "gpu_launches": launches_per_frame * args.steps,
+            "clocks": clk, "timed_loops": len(loop_ms), "launches_per_step": launches_per_frame,
+            "gpu_launches": launches_per_frame * args.steps * len(loop_ms),
         }
+        if multi:
+            line.update(multi)
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

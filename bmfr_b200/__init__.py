@@ -14,12 +14,14 @@ import ctypes as C
 
 import numpy as np
 
+from bmfr_scene import Scene  # the input source (its own library, libbmfr_scene.so)
+
 from . import _native
-from ._native import (BatchTuning, ServerConfig, ServerStats, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers, SceneDesc, Sizes, check,
-                      lib, PIPELINE_FUSED, PIPELINE_STAGED, QR_CHOLESKY2, QR_HOUSEHOLDER, QR_REFERENCE)
+from ._native import (BatchTuning, ServerConfig, ServerStats, BmfrError, FrameInputs, FrameIO, Params, PlanBuffers,
+                      Sizes, check, lib, PIPELINE_FUSED, PIPELINE_STAGED, QR_CHOLESKY2, QR_HOUSEHOLDER, QR_REFERENCE)
 
 __all__ = [
-    "Plan", "Batch", "Server", "Scene", "BmfrError", "default_params", "block_offsets",
+    "Plan", "Batch", "Server", "Router", "Scene", "BmfrError", "default_params", "block_offsets",
     "accumulate_noisy_data", "fitter", "fitter_fp64", "weighted_sum", "accumulate_filtered_data", "taa",
     "write_pfm", "read_pfm", "psnr",
     "PIPELINE_FUSED", "PIPELINE_STAGED", "QR_REFERENCE", "QR_CHOLESKY2", "QR_HOUSEHOLDER", "library_path",
@@ -523,6 +525,13 @@ class Server:
                                      C.byref(rid)), "bmfr_server_submit")
         return rid.value
 
+    def snapshot_bytes(self, sid: int) -> int:
+        """Size of an open stream's history snapshot."""
+        n = C.c_size_t()
+        check(lib.bmfr_batch_snapshot_bytes(lib.bmfr_server_batch(self.handle), int(sid), C.byref(n)),
+              "bmfr_batch_snapshot_bytes")
+        return n.value
+
     def snapshot_stream(self, sid: int, out, stream=None):
         """bmfr_server_snapshot_stream into `out` (host numpy uint8 array or
         device tensor, at least batch snapshot_bytes long)."""
@@ -556,69 +565,7 @@ class Server:
         check(lib.bmfr_server_set_tuning(self.handle, C.byref(t)), "bmfr_server_set_tuning")
 
 
-# -- input source ------------------------------------------------------------
-
-class Scene:
-    """Seeded procedural stand-in for the reference's EXR dataset and
-    camera_matrices.h (opencl/bmfr.cpp:44-53, 145-172)."""
-
-    def __init__(self, seed: int, width: int, height: int, sphere_count: int = 12, **overrides):
-        d = SceneDesc()
-        check(lib.bmfr_scene_default(C.byref(d), int(seed), int(width), int(height), int(sphere_count)),
-              "bmfr_scene_default")
-        for k, v in overrides.items():
-            if not hasattr(d, k):
-                raise AttributeError(f"unknown scene field {k!r}")
-            setattr(d, k, v)
-        self.desc = d
-        self.width, self.height = width, height
-
-    @property
-    def position_limit_squared(self) -> float:
-        return self.desc.position_limit_squared
-
-    @property
-    def normal_limit_squared(self) -> float:
-        return self.desc.normal_limit_squared
-
-    def camera(self, frame: int) -> np.ndarray:
-        m = np.empty(16, dtype=np.float32)
-        check(lib.bmfr_scene_camera(C.byref(self.desc), int(frame), m.ctypes.data_as(C.POINTER(C.c_float))),
-              "bmfr_scene_camera")
-        return m
-
-    def prev_camera(self, frame: int) -> np.ndarray:
-        """camera_matrices[max(frame - 1, 0)], the matrix frame `frame` uses
-        (opencl/bmfr.cpp:440-442)."""
-        return self.camera(max(frame - 1, 0))
-
-    def pixel_offset(self, frame: int) -> np.ndarray:
-        o = np.empty(2, dtype=np.float32)
-        check(lib.bmfr_scene_pixel_offset(C.byref(self.desc), int(frame), o.ctypes.data_as(C.POINTER(C.c_float))),
-              "bmfr_scene_pixel_offset")
-        return o
-
-    def render(self, frame: int, clean: bool = False, threads: int = 0) -> dict:
-        H, W = self.height, self.width
-        out = {k: np.empty((H, W, 3), dtype=np.float32) for k in ("albedo", "normals", "positions", "noisy")}
-        cl = np.empty((H, W, 3), dtype=np.float32) if clean else None
-        fp = C.POINTER(C.c_float)
-        check(lib.bmfr_scene_render(C.byref(self.desc), int(frame), out["albedo"].ctypes.data_as(fp),
-                                    out["normals"].ctypes.data_as(fp), out["positions"].ctypes.data_as(fp),
-                                    out["noisy"].ctypes.data_as(fp),
-                                    cl.ctypes.data_as(fp) if cl is not None else None, int(threads)),
-              "bmfr_scene_render")
-        if cl is not None:
-            out["clean"] = cl
-        return out
-
-    def render_device(self, frame: int, albedo, normals, positions, noisy, clean=None, stream=None) -> None:
-        """Renders frame `frame` on the GPU into device tensors (H*W*3 float32)."""
-        n = self.width * self.height * 12
-        check(lib.bmfr_scene_render_device(C.byref(self.desc), int(frame), _ptr(albedo, "albedo", n),
-                                           _ptr(normals, "normals", n), _ptr(positions, "positions", n),
-                                           _ptr(noisy, "noisy", n), _ptr(clean, "clean", n, optional=True),
-                                           _stream_ptr(stream)), "bmfr_scene_render_device")
+from .router import Router  # noqa: E402  (per-GPU servers behind one placement)
 
 
 # -- image output (include/bmfr_image.h) -----------------------------------

@@ -1,4 +1,4 @@
-"""ctypes binding of libbmfr_b200.so (include/bmfr_b200.h, bmfr_batch.h, bmfr_scene.h, bmfr_image.h).
+"""ctypes binding of libbmfr_b200.so (include/bmfr_b200.h, bmfr_batch.h, bmfr_image.h).
 
 The library is the product: importing this module loads it and raises if it
 is missing — there is no fallback implementation.
@@ -98,19 +98,6 @@ class ServerStats(C.Structure):
                 ("elapsed_seconds", C.c_double)]
 
 
-class SceneDesc(C.Structure):
-    _fields_ = [
-        ("seed", C.c_uint64), ("width", C.c_int), ("height", C.c_int),
-        ("sphere_count", C.c_int), ("orbit_degrees_per_frame", C.c_float),
-        ("orbit_start_degrees", C.c_float), ("orbit_radius", C.c_float),
-        ("camera_height", C.c_float), ("vertical_fov_degrees", C.c_float),
-        ("noise_mu", C.c_float), ("noise_sigma", C.c_float),
-        ("firefly_fraction", C.c_float), ("firefly_scale", C.c_float),
-        ("plane_half_extent", C.c_float), ("position_limit_squared", C.c_float),
-        ("normal_limit_squared", C.c_float),
-    ]
-
-
 def _load() -> C.CDLL:
     if not _LIB_PATH.exists():
         raise ImportError(
@@ -129,6 +116,8 @@ def _load() -> C.CDLL:
         "bmfr_fitter": (i, [vp, vp, vp, vp, i, vp]),
         "bmfr_fitter_fp64": (i, [vp, vp, vp, vp, i, vp]),
         "bmfr_fitter_noalloc": (i, [C.POINTER(Params), i, i, vp, vp, vp, i, vp]),
+        "bmfr_fitter_noalloc_check": (i, [vp]),
+        "bmfr_fitter_noalloc_probe_bounded_wait": (i, [C.c_uint, vp]),
         "bmfr_weighted_sum": (i, [vp, vp, vp, vp, vp, vp, vp, i, vp]),
         "bmfr_accumulate_filtered_data": (i, [vp, vp, vp, u8p, vp, vp, u8p, vp, vp, i, vp]),
         "bmfr_taa": (i, [vp, vp, vp, vp, vp, i, vp]),
@@ -180,11 +169,6 @@ def _load() -> C.CDLL:
         "bmfr_server_set_tuning": (i, [vp, C.POINTER(BatchTuning)]),
         "bmfr_last_error": (C.c_char_p, []),
         "bmfr_status_string": (C.c_char_p, [i]),
-        "bmfr_scene_default": (i, [C.POINTER(SceneDesc), C.c_uint64, i, i, i]),
-        "bmfr_scene_camera": (i, [C.POINTER(SceneDesc), i, fp]),
-        "bmfr_scene_pixel_offset": (i, [C.POINTER(SceneDesc), i, fp]),
-        "bmfr_scene_render": (i, [C.POINTER(SceneDesc), i, fp, fp, fp, fp, fp, i]),
-        "bmfr_scene_render_device": (i, [C.POINTER(SceneDesc), i, vp, vp, vp, vp, vp, vp]),
         "bmfr_write_pfm": (i, [C.c_char_p, i, i, fp]),
         "bmfr_read_pfm": (i, [C.c_char_p, C.POINTER(i), C.POINTER(i), fp, C.c_size_t]),
         "bmfr_psnr": (C.c_double, [fp, fp, C.c_size_t, f]),

@@ -1,9 +1,12 @@
-"""Build recipe of the in-tree native library bmfr_b200/libbmfr_b200.so.
+"""Build recipe of the in-tree native libraries: bmfr_b200/libbmfr_b200.so
+(the denoising pipeline) and bmfr_scene/libbmfr_scene.so (the procedural
+input source, kept apart so that code that only needs inputs maps no
+pipeline code).
 
 CUDA sources are compiled by nvcc for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a); host C++ sources by the system
-g++ with OpenMP.  Objects go to bmfr_b200/_build/ and are rebuilt when a
-source or header is newer.  Run ``python bmfr_b200/build.py``.
+g++ with OpenMP.  Objects go to each package's _build/ and are rebuilt when
+a source or header is newer.  Run ``python bmfr_b200/build.py``.
 """
 from __future__ import annotations
 
@@ -20,6 +23,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libbmfr_b200.so"
+SCENE_PKG = ROOT / "bmfr_scene"
+SCENE_LIB = SCENE_PKG / "libbmfr_scene.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -37,12 +42,12 @@ def _gxx() -> str:
 
 
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
-                     "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}"]
-GXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", f"-I{INCLUDE}", f"-I{CSRC}"]
+                     "-Xptxas", "-warn-spills", f"-I{INCLUDE}"]
+GXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", f"-I{INCLUDE}"]
 
 
-def _headers() -> list[Path]:
-    return sorted(list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h")))
+def _headers(csrc: Path) -> list[Path]:
+    return sorted(list(csrc.glob("*.cuh")) + list(csrc.glob("*.h")) + list(INCLUDE.glob("*.h")))
 
 
 def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
@@ -52,14 +57,15 @@ def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
     return any(p.stat().st_mtime > t for p in [src, *deps])
 
 
-def _compile(src: Path, verbose: bool) -> Path:
-    obj = BUILD / (src.name + ".o")
-    if not _stale(obj, src, _headers()):
+def _compile(src: Path, build: Path, verbose: bool) -> Path:
+    csrc = src.parent
+    obj = build / (src.name + ".o")
+    if not _stale(obj, src, _headers(csrc)):
         return obj
     if src.suffix == ".cu":
-        cmd = [_nvcc(), "-ccbin", _gxx(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [_nvcc(), "-ccbin", _gxx(), *NVCC_FLAGS, f"-I{csrc}", "-c", str(src), "-o", str(obj)]
     else:
-        cmd = [_gxx(), *GXX_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [_gxx(), *GXX_FLAGS, f"-I{csrc}", "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -68,21 +74,27 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
-def build(verbose: bool = False) -> Path:
-    """Compiles and links libbmfr_b200.so; returns its path."""
-    BUILD.mkdir(exist_ok=True)
-    sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+def _build_lib(csrc: Path, build: Path, lib: Path, verbose: bool) -> Path:
+    build.mkdir(exist_ok=True)
+    sources = sorted(csrc.glob("*.cu")) + sorted(csrc.glob("*.cpp"))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), sources))
-    if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        cmd = [_nvcc(), "-ccbin", _gxx(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs),
+        objs = list(ex.map(lambda s: _compile(s, build, verbose), sources))
+    if not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        cmd = [_nvcc(), "-ccbin", _gxx(), *ARCH, "-shared", "-o", str(lib), *map(str, objs),
                "-Xcompiler", "-fopenmp", "-lgomp", "-cudart", "static"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f"linking {LIB.name} failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+            raise RuntimeError(f"linking {lib.name} failed:\n{r.stdout}\n{r.stderr}")
+    return lib
+
+
+def build(verbose: bool = False) -> Path:
+    """Compiles and links libbmfr_b200.so and libbmfr_scene.so; returns the
+    pipeline library's path."""
+    _build_lib(SCENE_PKG / "csrc", SCENE_PKG / "_build", SCENE_LIB, verbose)
+    return _build_lib(CSRC, BUILD, LIB, verbose)
 
 
 def build_oracle(verbose: bool = False) -> Path:
@@ -96,18 +108,18 @@ def build_oracle(verbose: bool = False) -> Path:
     return oracle / "libbmfr_oracle.so"
 
 
-REFERENCE_CL = Path("/root/reference/opencl/bmfr.cl")
-
-
-def build_reference(verbose: bool = False) -> Path | None:
+def build_reference(reference_cl: str | os.PathLike | None = None, verbose: bool = False) -> Path | None:
     """Compiles the reference's own kernels for the CPU (test
-    infrastructure: oracle/ref_cl -> oracle/_ref/libbmfr_ref.so) when the
-    reference source is present; otherwise keeps a library built earlier."""
+    infrastructure: oracle/ref_cl -> oracle/_ref/libbmfr_ref.so) from the
+    reference's opencl/bmfr.cl, given as `reference_cl` or by the
+    environment variable BMFR_REFERENCE_CL; without that source, keeps a
+    library built earlier."""
     oracle = ROOT / "oracle"
-    if not REFERENCE_CL.exists():
+    src = reference_cl or os.environ.get("BMFR_REFERENCE_CL")
+    if not src or not Path(src).exists():
         lib = oracle / "_ref" / "libbmfr_ref.so"
         return lib if lib.exists() else None
-    r = subprocess.run(["make", "-C", str(oracle), "ref", f"REF_SRC={REFERENCE_CL}", f"PYTHON={sys.executable}"],
+    r = subprocess.run(["make", "-C", str(oracle), "ref", f"REF_SRC={src}", f"PYTHON={sys.executable}"],
                        capture_output=True, text=True)
     if verbose:
         print(r.stdout, r.stderr)
@@ -119,4 +131,4 @@ def build_reference(verbose: bool = False) -> Path | None:
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))
     print(build_oracle(verbose="-v" in sys.argv))
-    print(build_reference(verbose="-v" in sys.argv))
+    print(build_reference(verbose="-v" in sys.argv))   # with BMFR_REFERENCE_CL set

@@ -352,6 +352,34 @@ int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height, float*
     return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter_noalloc launch");
 }
 
+int bmfr_fitter_noalloc_check(void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    int* status = nullptr;
+    cudaError_t e = bmfr::static_fitter_status(&status, s);
+    if (e != cudaSuccess) return cuda_fail(e, "fitter_noalloc_check");
+    int v = 0;
+    e = cudaMemcpyAsync(&v, status, sizeof v, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "fitter_noalloc_check");
+    if (v != 0) {
+        e = cudaMemsetAsync(status, 0, sizeof(int), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_fail(e, "fitter_noalloc_check");
+        return fail(BMFR_E_TIMEOUT, "a bmfr_fitter_noalloc kernel's bounded wait ran out (device status " +
+                                        std::to_string(v) + ")");
+    }
+    return BMFR_OK;
+}
+
+int bmfr_fitter_noalloc_probe_bounded_wait(unsigned int limit_us, void* stream) {
+    if (limit_us < 1 || limit_us > 1000000) return fail(BMFR_E_INVALID, "limit_us must be within [1, 1000000]");
+    cudaStream_t s = (cudaStream_t)stream;
+    int* status = nullptr;
+    cudaError_t e = bmfr::static_fitter_status(&status, s);
+    if (e == cudaSuccess) e = bmfr::launch_bounded_wait_probe(status, 1000ull * limit_us, s);
+    return e == cudaSuccess ? BMFR_OK : cuda_fail(e, "fitter_noalloc_probe_bounded_wait");
+}
+
 int bmfr_weighted_sum(const bmfr_plan* plan, const float* weights, const float* mins_maxs, float* output,
                       const float* current_normals, const float* current_positions, const float* current_noisy,
                       int frame_number, void* stream) {

@@ -82,8 +82,6 @@ __device__ __forceinline__ int mirror(int i, int n) {
     return i;
 }
 
-// convert_int_rtn with defined results: NaN and magnitudes beyond 2^30 map to
-// +-2^30, outside every image.
 // Programmatic dependent launch.  The pipeline's kernels are launched with
 // programmatic stream serialization (launch_chained), so a kernel's launch
 // is processed while the kernel before it in the stream drains; before it
@@ -96,6 +94,8 @@ __device__ __forceinline__ void await_previous_kernel() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// convert_int_rtn with defined results: NaN and magnitudes beyond 2^30 map to
+// +-2^30, outside every image.
 __device__ __forceinline__ int floor_to_int(float v) {
     if (!(v == v)) return -(1 << 30);
     const float f = floorf(v);

@@ -22,6 +22,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -199,12 +200,16 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
                                    float* mins_maxs, const float* noise, int* status, cudaStream_t s) {
     auto kern = k_fitter<HALF_TMP, METHOD, NOISE_GLOBAL>;
     const int smem = (int)sizeof(FitterShared<HALF_TMP, NOISE_GLOBAL>) + 1024;   // + alignment slack
-    static int grid_cap[64] = {0};   // per device
+    // Resident CTAs per device, found once per device and instantiation.
+    // Threads that race on the first call compute the same value, so a
+    // relaxed atomic store and load are enough.
+    static std::atomic<int> grid_cap[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (grid_cap[dev] == 0) {
+    int cap = grid_cap[dev].load(std::memory_order_relaxed);
+    if (cap == 0) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         int per_sm = 0, sms = 0;
@@ -212,9 +217,10 @@ static cudaError_t launch_fitter_t(int nblocks, int frame, NoiseConst nc, const 
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
-        grid_cap[dev] = (per_sm > 0 ? per_sm : 1) * sms;
+        cap = (per_sm > 0 ? per_sm : 1) * sms;
+        grid_cap[dev].store(cap, std::memory_order_relaxed);
     }
-    const int grid = nblocks < grid_cap[dev] ? nblocks : grid_cap[dev];
+    const int grid = nblocks < cap ? nblocks : cap;
     if (grid <= 0) return cudaSuccess;
     CUtensorMap map;
     std::memset(&map, 0, sizeof map);
@@ -266,7 +272,10 @@ cudaError_t launch_fitter(const Geometry& g, int frame, NoiseConst nc, const voi
 // grow with the image: this fixed size serves every image size a plan
 // accepts.  In host code g_fitter_scratch only names the symbol; the device
 // address comes from cudaGetSymbolAddress, taken once per device with that
-// device current.
+// device current, when the status word is also cleared (on the caller's
+// stream, ordered before the call's kernels).  From then on the word is
+// sticky: a kernel that gives up a bounded wait sets it, and only
+// static_fitter_status_clear (bmfr_fitter_noalloc_check) clears it.
 constexpr size_t kStaticStatusOffset = kNoiseTableBytes;             // 36,864
 constexpr size_t kStaticScratchBytes = kStaticStatusOffset + 256;    // table + status word
 static __device__ __align__(256) unsigned char g_fitter_scratch[kStaticScratchBytes];
@@ -274,7 +283,7 @@ static __device__ __align__(256) unsigned char g_fitter_scratch[kStaticScratchBy
 static std::mutex g_scratch_mutex;
 static void* g_scratch_address[64] = {nullptr};
 
-static cudaError_t static_scratch_address(void** out) {
+static cudaError_t static_scratch_address(void** out, cudaStream_t s) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -284,22 +293,30 @@ static cudaError_t static_scratch_address(void** out) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_fitter_scratch);
         if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(static_cast<unsigned char*>(p) + kStaticStatusOffset, 0, sizeof(int), s);
+        if (e != cudaSuccess) return e;
         g_scratch_address[dev] = p;
     }
     *out = g_scratch_address[dev];
     return cudaSuccess;
 }
 
+cudaError_t static_fitter_status(int** status, cudaStream_t s) {
+    void* base = nullptr;
+    const cudaError_t e = static_scratch_address(&base, s);
+    if (e != cudaSuccess) return e;
+    *status = reinterpret_cast<int*>(static_cast<unsigned char*>(base) + kStaticStatusOffset);
+    return cudaSuccess;
+}
+
 cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
                                  int qr, float* weights, float* mins_maxs, cudaStream_t s) {
     void* base = nullptr;
-    cudaError_t e = static_scratch_address(&base);
+    cudaError_t e = static_scratch_address(&base, s);
     if (e != cudaSuccess) return e;
     float* table = static_cast<float*>(base);
     int* status = reinterpret_cast<int*>(static_cast<unsigned char*>(base) + kStaticStatusOffset);
-    e = cudaMemsetAsync(status, 0, sizeof(int), s);   // the array keeps the last call's contents
-    if (e != cudaSuccess) return e;
-    e = launch_noise_table(frame, table, s);
+    e = launch_noise_table(frame, table, s);   // rewrites the table the last call left
     if (e != cudaSuccess) return e;
     return launch_fitter(g, frame, nc, tmp, half_tmp, qr, weights, mins_maxs, table, status, s);
 }

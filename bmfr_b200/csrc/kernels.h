@@ -56,6 +56,9 @@ cudaError_t launch_bounded_wait_probe(int* status, unsigned long long limit_ns, 
 // The fitter with its scratch in a static device array (no allocation).
 cudaError_t launch_fitter_static(const Geometry& g, int frame, NoiseConst nc, const void* tmp, bool half_tmp,
                                  int qr, float* weights, float* mins_maxs, cudaStream_t s);
+// Device address of that array's bounded-wait status word (set-up on first
+// use per device, ordered on `s`).
+cudaError_t static_fitter_status(int** status, cudaStream_t s);
 constexpr size_t kNoiseTableBytes = 9 * 4 * 256 * sizeof(float);
 
 cudaError_t launch_weighted_sum(const Geometry& g, int frame, const float* weights, const float* mins_maxs,

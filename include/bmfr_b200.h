@@ -178,11 +178,22 @@ int bmfr_fitter_fp64(const bmfr_plan* plan, double* weights, float* mins_maxs,
  * address (cudaGetSymbolAddress) with the device current; make that first
  * call before any stream capture.  All calls share the array and each call
  * rewrites it, so calls whose kernels overlap on the GPU (different streams,
- * or one stream and another without ordering) race: order them.  Results
- * equal bmfr_fitter's. */
+ * or one stream and another without ordering) race: order them.  The
+ * weights and min/max values are bit for bit those of bmfr_fitter (the same
+ * arithmetic).  A bounded wait that runs out is recorded in the array's
+ * status word, which no call clears; bmfr_fitter_noalloc_check reads it. */
 int bmfr_fitter_noalloc(const bmfr_params* params, int width, int height,
                         float* weights, float* mins_maxs, const void* tmp_data,
                         int frame_number, void* stream);
+/* Waits for `stream` and reports whether a bmfr_fitter_noalloc kernel on the
+ * current device gave up a bounded wait since the last check
+ * (BMFR_E_TIMEOUT; the status word is then cleared).  Allocates nothing. */
+int bmfr_fitter_noalloc_check(void* stream);
+/* Diagnostics of that failure path, as bmfr_plan_probe_bounded_wait for a
+ * plan: one CTA whose bounded wait (limit_us, 1..1,000,000) on a barrier
+ * that nothing completes runs out and records the timeout in the static
+ * array's status word; no fault, trap or endless wait is involved. */
+int bmfr_fitter_noalloc_probe_bounded_wait(unsigned int limit_us, void* stream);
 
 /* weighted_sum (bmfr.cl:703-758). current_noisy is unused, as in the
  * reference (debug only, bmfr.cl:709), and may be NULL. */

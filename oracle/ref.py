@@ -8,7 +8,9 @@ reference host program's frame loop over the reference's kernels.  The tests
 use it to pin the oracle restatement and to write the golden fixtures.
 
 The library is built from the reference's source where it lies (`make -C
-oracle ref`); without that source, only a library built earlier can be used.
+oracle ref REF_SRC=<opencl/bmfr.cl>`, or BMFR_REFERENCE_CL set in the
+environment when this module loads it); without that source, only a library
+built earlier can be used.
 """
 from __future__ import annotations
 
@@ -22,20 +24,23 @@ from .oracle import Oracle, Cfg, _p, FITTER_REFERENCE
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
 LIB = REF_DIR / "libbmfr_ref.so"
-DEFAULT_SOURCE = Path(os.environ.get("BMFR_REFERENCE_CL", "/root/reference/opencl/bmfr.cl"))
+def _source() -> Path | None:
+    """The reference's opencl/bmfr.cl named by BMFR_REFERENCE_CL, if it exists."""
+    src = os.environ.get("BMFR_REFERENCE_CL")
+    return Path(src) if src and Path(src).exists() else None
 
 
 def available() -> bool:
     """True if the library exists or can be built from the reference source."""
-    return LIB.exists() or DEFAULT_SOURCE.exists()
+    return LIB.exists() or _source() is not None
 
 
 def build() -> Path:
     """Builds oracle/_ref/libbmfr_ref.so from the reference's kernel source."""
-    if not DEFAULT_SOURCE.exists():
-        raise FileNotFoundError(f"reference kernel source not found: {DEFAULT_SOURCE}")
-    subprocess.run(["make", "-C", str(HERE), "ref", f"REF_SRC={DEFAULT_SOURCE}"], check=True,
-                   capture_output=True)
+    src = _source()
+    if src is None:
+        raise FileNotFoundError("reference kernel source not found: set BMFR_REFERENCE_CL to its opencl/bmfr.cl")
+    subprocess.run(["make", "-C", str(HERE), "ref", f"REF_SRC={src}"], check=True, capture_output=True)
     return LIB
 
 
@@ -45,7 +50,7 @@ _lib = None
 def _load() -> C.CDLL:
     global _lib
     if _lib is None:
-        if DEFAULT_SOURCE.exists():
+        if _source() is not None:
             build()          # make: a no-op when the library is current
         if not LIB.exists():
             raise FileNotFoundError(f"{LIB} is not built and the reference source is absent")

@@ -38,9 +38,13 @@ def device_array(ptr, shape, dtype):
 
 
 @pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
+# 128x96 over 17 frames: every entry of the device's BLOCK_OFFSETS table
+# (frame % 16, opencl/bmfr.cl:267-285) and the wrap back to entry 0.
 # 1280x720: 984 blocks, more than the persistent fitter's CTAs, so each CTA
 # fits several blocks through both tile buffers and both barrier phases.
-@pytest.mark.parametrize("W,H,frames", [(128, 96, 6), (256, 256, 8), (197, 131, 5), (1280, 720, 3)])
+# 1920x1080 and 3840x2160: the precision and many-stream workloads' sizes.
+@pytest.mark.parametrize("W,H,frames", [(128, 96, 17), (256, 256, 8), (197, 131, 5), (1280, 720, 3),
+                                        (1920, 1080, 2), (3840, 2160, 1)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     import torch
     sc = B.Scene(21, W, H, 12)

@@ -46,8 +46,9 @@ def test_fp64_fitter_matches_oracle(cuda):
 
 
 # 1280x720: more blocks than the persistent fitter's CTAs (each CTA fits
-# several blocks through both tile buffers).
-@pytest.mark.parametrize("W,H", [(256, 192), (1280, 720)])
+# several blocks through both tile buffers); 1920x1080: the precision
+# workload's size.
+@pytest.mark.parametrize("W,H", [(256, 192), (1280, 720), (1920, 1080)])
 @pytest.mark.parametrize("qr", [B.QR_CHOLESKY2, B.QR_HOUSEHOLDER])
 def test_fp32_qr_weights_against_fp64(cuda, qr, W, H):
     import torch
@@ -84,6 +85,29 @@ def test_precision_form_output_against_fp64(cuda, pipeline, qr):
     plan = B.Plan(W, H, fp32_qr=qr, half_history=1, pipeline=pipeline,
                   position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
     for f in range(6):
+        d = sc.render(f)
+        want = ref.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f),
+                        sc.pixel_offset(f))
+        plan.upload_frame(d["albedo"], d["normals"], d["positions"], d["noisy"])
+        plan.denoise_frame(sc.prev_camera(f), sc.pixel_offset(f))
+        e = rel_err(plan.download_result(), want)
+        assert e.mean() < 2e-4, (f, e.mean())
+        assert (e > 1e-3).mean() <= 1e-3, (f, (e > 1e-3).mean())
+        assert e.max() < 2e-2, (f, e.max())
+    plan.close()
+
+
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
+def test_precision_form_at_1080p_against_fp64(cuda, pipeline):
+    """The precision workload (1920x1080, 24 spheres, its own seed): binary16
+    histories and CholeskyQR2 against the pipeline with the fp64 fitter and
+    float histories, with the bounds above."""
+    W, H = 1920, 1080
+    sc = B.Scene(20240603, W, H, 24)
+    ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared), fitter_mode=FITTER_FP64)
+    plan = B.Plan(W, H, fp32_qr=B.QR_CHOLESKY2, half_history=1, pipeline=pipeline,
+                  position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
+    for f in range(3):
         d = sc.render(f)
         want = ref.step(d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f),
                         sc.pixel_offset(f))

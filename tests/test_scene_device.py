@@ -1,0 +1,61 @@
+"""The on-device G-buffer generator (bmfr_scene_render_device) against the
+host renderer (bmfr_scene_render) that every parity test feeds the oracle.
+
+The batched and served benchmarks render their inputs on the GPU, so this
+pins those inputs to the host stream.  The two are not bit-identical, by
+construction, and the tolerances below follow from how they differ:
+
+* the device casts rays in float, the host in double, so positions and
+  normals of a pixel that hits the same object agree to float rounding of
+  a ray of length ~10: |dp| <= 1e-4 (1 + |p|), |dn| <= 1e-4;
+* a grazing ray at an object's silhouette may hit another object (or
+  nothing) in one of them: such pixels are counted (albedo differs, or one
+  side misses) and must stay below 0.2 % of the image;
+* the noise draws come from the same 64-bit counter hash, as a 24-bit
+  uniform on the device and a 53-bit one on the host; Box-Muller's log and
+  cos then agree to ~1e-6 except where the uniform is tiny (the far tail of
+  the lognormal), so the 1-spp colour is within 1e-3 relative for 99.99 % of
+  the channels, and a firefly decision (a uniform below 0.001, a factor of
+  100 when it differs) may differ only where a uniform lies within 2^-24 of
+  the threshold: at most 1e-5 of the channels are off by more than 10 %;
+* the albedo is copied from the same table: exact where the object agrees.
+"""
+import numpy as np
+import pytest
+
+import bmfr_b200 as B
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("W,H,frames", [(256, 192, (0, 1, 7)), (1280, 720, (0, 30))])
+def test_device_render_matches_host_render(cuda, W, H, frames):
+    import torch
+    sc = B.Scene(77, W, H, 16)
+    n = W * H * 3
+    dev = {k: torch.empty(n, dtype=torch.float32, device=cuda)
+           for k in ("albedo", "normals", "positions", "noisy", "clean")}
+    for f in frames:
+        host = sc.render(f, clean=True)
+        sc.render_device(f, dev["albedo"], dev["normals"], dev["positions"], dev["noisy"], clean=dev["clean"])
+        torch.cuda.synchronize()
+        got = {k: v.cpu().numpy().reshape(H, W, 3) for k, v in dev.items()}
+        hit_h = np.any(host["normals"] != 0, axis=-1)
+        hit_d = np.any(got["normals"] != 0, axis=-1)
+        same = (hit_h == hit_d) & np.all(host["albedo"] == got["albedo"], axis=-1)
+        assert hit_h.mean() > 0.3, "the scene must cover a good part of the image"
+        assert (~same).mean() < 2e-3, f"frame {f}: {(~same).mean():.2e} of pixels hit different objects"
+        m = same & hit_h
+        dp = np.abs(got["positions"] - host["positions"])[m]
+        assert (dp <= 1e-4 * (1.0 + np.abs(host["positions"][m]))).all(), f"frame {f}: positions {dp.max():.2e}"
+        dn = np.abs(got["normals"] - host["normals"])[m]
+        assert dn.max() <= 1e-4, f"frame {f}: normals {dn.max():.2e}"
+        # Misses are all zero on both sides.
+        miss = same & ~hit_h
+        for k in ("albedo", "normals", "positions", "noisy", "clean"):
+            assert (got[k][miss] == 0).all() and (host[k][miss] == 0).all(), k
+        rel = np.abs(got["noisy"] - host["noisy"])[m] / np.maximum(np.abs(host["noisy"][m]), 1e-6)
+        assert np.quantile(rel, 0.9999) <= 1e-3, f"frame {f}: noisy {np.quantile(rel, 0.9999):.2e}"
+        assert (rel > 0.1).mean() <= 1e-5, f"frame {f}: {(rel > 0.1).sum()} channels off by more than 10 %"
+        dc = np.abs(got["clean"] - host["clean"])[m]
+        assert dc.max() <= 1e-4, f"frame {f}: clean {dc.max():.2e}"

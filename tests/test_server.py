@@ -110,3 +110,45 @@ def test_stream_moves_between_servers(cuda):
         np.testing.assert_array_equal(got[k].cpu().numpy(), want[k].cpu().numpy(), err_msg=f"frame {3 + k}")
     one.close()
     two.close()
+
+
+def test_router_over_two_servers_places_and_migrates(cuda):
+    """The host-side router over two servers (two GPUs' worth, here on one
+    device): streams go where the budget has room, requests follow their
+    stream, and a stream moved between servers mid-sequence gives the frames
+    its own plan gives."""
+    import torch
+    params = B.default_params(pipeline=B.PIPELINE_STAGED, fp32_qr=1, half_history=1)
+    one_stream = B.Batch.stream_bytes(params, 200, 120)
+    router = B.Router([B.Server(params), B.Server(params)], budget_bytes=2 * one_stream,
+                      stream_bytes=lambda w, h: B.Batch.stream_bytes(params, w, h))
+    streams = [Stream(80 + k, 200, 120, params, cuda) for k in range(3)]
+    ids = [router.open_stream(s.w, s.h) for s in streams]
+    assert sorted(router.gpu_of(i) for i in ids) == [0, 0, 1]
+    outs = {}
+
+    def submit(k, f):
+        s = streams[k]
+        out = torch.empty(s.w * s.h * 3, dtype=torch.float32, device=cuda)
+        io = s.io(f)
+        io.result = out.data_ptr()
+        router.submit(ids[k], s.sc.prev_camera(f), s.sc.pixel_offset(f), io=io)
+        outs[(k, f)] = out
+
+    for f in range(2):
+        for k in range(3):
+            submit(k, f)
+    moved = next(i for i, g in enumerate(router.gpu_of(x) for x in ids) if g == 0)
+    assert router.migrate(ids[moved]) == 1               # the other server had room for one more
+    for f in range(2, 4):
+        for k in range(3):
+            submit(k, f)
+    router.drain()
+    torch.cuda.synchronize()
+    for k, s in enumerate(streams):
+        for f in range(4):
+            np.testing.assert_array_equal(outs[(k, f)].cpu().numpy(), s.plan_step(f).cpu().numpy(),
+                                          err_msg=f"stream {k} frame {f}")
+    router.close()
+    for srv in router.servers:
+        srv.close()
