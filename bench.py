@@ -86,6 +86,10 @@ def stage_bytes(w, h):
         # acc_cur, tone_mapped written (float histories)
         "weighted_sum+accumulate_filtered_data": 94 * P,
         "taa": 44 * P,
+        # one kernel: N, P, prev_pix, accept, albedo, spp, the filtered and
+        # TAA histories read; both histories written (float histories); the
+        # tone-mapped frame stays on chip
+        "weighted_sum+accumulate_filtered_data+taa": 94 * P,
         "noise_table": 9 * 4 * 256 * 4,
         # accumulate (95 B/px + 26 B read per margin pixel from the inputs, no
         # tmp_data) + weighted sum and filtered accumulation (82 B/px less the

@@ -218,7 +218,7 @@ class Plan:
         check(lib.bmfr_plan_probe_bounded_wait(self.handle, int(limit_us), _stream_ptr(stream)),
               "bmfr_plan_probe_bounded_wait")
 
-    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data", None, "taa")
+    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data+taa", None, None)
     FUSED_STAGES = ("noise_table", "block_kernel", None, None, "taa")
 
     def stage_times(self) -> dict:
@@ -228,6 +228,11 @@ class Plan:
         check(lib.bmfr_plan_stage_times(self.handle, ms), "bmfr_plan_stage_times")
         names = self.FUSED_STAGES if self.params.pipeline == PIPELINE_FUSED else self.STAGES
         return {n: float(v) for n, v in zip(names, ms) if n is not None}
+
+    def keep_intermediates(self, enable: bool = True) -> None:
+        """Staged pipeline: also write the filtered and tone-mapped frames
+        of every frame (for inspection; outputs are unchanged)."""
+        check(lib.bmfr_plan_keep_intermediates(self.handle, int(enable)), "bmfr_plan_keep_intermediates")
 
     def buffers(self) -> PlanBuffers:
         b = PlanBuffers()
@@ -455,8 +460,8 @@ class Batch:
         check(lib.bmfr_batch_get_tuning(self.handle, C.byref(t)), "bmfr_batch_get_tuning")
         return t
 
-    def set_tuning(self, block_ctas_per_sm=0, taa_tile_w=30, taa_tile_h=32, staging_depth=0) -> None:
-        t = BatchTuning(block_ctas_per_sm, taa_tile_w, taa_tile_h, staging_depth)
+    def set_tuning(self, block_ctas_per_sm=0, taa_tile_w=30, taa_tile_h=32, staging_depth=0, pixel_pass=0) -> None:
+        t = BatchTuning(block_ctas_per_sm, taa_tile_w, taa_tile_h, staging_depth, pixel_pass)
         check(lib.bmfr_batch_set_tuning(self.handle, C.byref(t)), "bmfr_batch_set_tuning")
 
     def autotune(self, slots, matrices, offsets, io=None, steps=3, stream=None):

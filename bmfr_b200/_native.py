@@ -80,7 +80,7 @@ class FrameIO(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("block_ctas_per_sm", C.c_int), ("taa_tile_w", C.c_int), ("taa_tile_h", C.c_int),
-                ("staging_depth", C.c_int)]
+                ("staging_depth", C.c_int), ("pixel_pass", C.c_int)]
 
 
 class ServerConfig(C.Structure):
@@ -130,6 +130,7 @@ def _load() -> C.CDLL:
         "bmfr_plan_frame_number": (i, [vp]),
         "bmfr_plan_reset": (i, [vp]),
         "bmfr_plan_buffers_get": (i, [vp, C.POINTER(PlanBuffers)]),
+        "bmfr_plan_keep_intermediates": (i, [vp, i]),
         "bmfr_plan_enable_profiling": (i, [vp, i]),
         "bmfr_plan_check_device": (i, [vp, vp]),
         "bmfr_plan_probe_bounded_wait": (i, [vp, C.c_uint, vp]),

@@ -2,9 +2,10 @@
 //
 // The fused step: one frame of every participating stream, the streams'
 // 32x32 blocks forming one global queue that a single persistent launch of
-// the fused block kernel walks (accumulate + fit + weighted sum + filtered
-// accumulation per block, fused_block.cuh), then one launch over the
-// streams' TAA tiles.  Both read the step's description from device memory,
+// the fused block kernel walks (accumulate + fit, and with the pixel pass
+// off weighted sum + filtered accumulation, per block, fused_block.cuh),
+// then one launch over the streams' image tiles: TAA, or with the pixel
+// pass weighted sum + filtered accumulation + TAA (wsacc_taa_tile).  Both read the step's description from device memory,
 // so one captured CUDA graph serves every step.  (The staged step runs the
 // plan's kernels per stream, batch_host.cu.)
 #include <type_traits>
@@ -80,7 +81,8 @@ __global__ void __launch_bounds__(256) k_batch_noise(const BatchStepDesc* __rest
 // depth 0: blocks are taken from a global atomic queue; depth > 0: block
 // blockIdx.x + k * gridDim.x, with the inputs of the CTA's next `depth`
 // blocks prefetched into L2 while it fits the current one.
-template <int METHOD, bool HALF_TMP, typename HistT>
+// PIXELS: see fused_block_body.
+template <int METHOD, bool HALF_TMP, typename HistT, bool PIXELS>
 __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32) ? 3 : 2)
     k_batch_blocks(const BatchStepDesc* __restrict__ d, int* __restrict__ counter, int depth) {
     __shared__ FitterSmem sm;
@@ -95,7 +97,8 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
             const int ahead = item + depth * (int)gridDim.x;
             if (threadIdx.x < 32 && ahead < nb) prefetch_block_inputs(d, ahead);
             const int s = stream_of_block(d, item);
-            fused_block_body<METHOD, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
+            fused_block_body<METHOD, HALF_TMP, HistT, PIXELS>(d->s[s].job, item - d->s[s].block_start, sm, w_s,
+                                                              mm_s);
             __syncthreads();
         }
     } else {
@@ -105,7 +108,8 @@ __global__ void __launch_bounds__(256, (HALF_TMP && METHOD != kFitHouseholder32)
             const int item = item_s;
             if (item >= nb) break;
             const int s = stream_of_block(d, item);
-            fused_block_body<METHOD, HALF_TMP, HistT>(d->s[s].job, item - d->s[s].block_start, sm, w_s, mm_s);
+            fused_block_body<METHOD, HALF_TMP, HistT, PIXELS>(d->s[s].job, item - d->s[s].block_start, sm, w_s,
+                                                              mm_s);
             __syncthreads();
         }
     }
@@ -128,6 +132,25 @@ __global__ void __launch_bounds__(128) k_batch_taa(const BatchStepDesc* __restri
     }
 }
 
+// weighted_sum + accumulate_filtered_data + taa over every stream's image
+// tiles of kWtTileW x kWtTileH (the step's tiles with the pixel pass).
+template <typename HistT>
+__global__ void __launch_bounds__(256, 4) k_batch_wsacc_taa(const BatchStepDesc* __restrict__ d) {
+    __shared__ float4 s_ycc[kWtRingPixels], s_rgb[kWtRingPixels];
+    const int nt = d->n_tiles;
+    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+        const int s = stream_of_tile(d, tile);
+        const BatchStreamJob& J = d->s[s];
+        const FusedBuffers& fb = J.job.fb;
+        const int t = tile - J.tile_start;
+        wsacc_taa_tile<HistT>(J.job.g, J.job.a.frame, J.job.second_alpha, J.taa_alpha, fb.weights, fb.mins_maxs,
+                              fb.cur_n, fb.cur_p, fb.prev_pix, fb.accept, fb.albedo, fb.cur_spp,
+                              (const HistT*)fb.acc_prev, (HistT*)fb.acc_cur, nullptr, nullptr,
+                              (HistT*)J.result_hist, (const HistT*)J.result_prev, J.result_out,
+                              (t % J.tiles_x) * kWtTileW, (t / J.tiles_x) * kWtTileH, s_ycc, s_rgb);
+    }
+}
+
 cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaStream_t s) {
     const int grid = (max_streams * kNoiseTableFloats + 255) / 256;
     k_batch_noise<<<grid < 1184 ? grid : 1184, 256, 0, s>>>(desc);
@@ -135,15 +158,18 @@ cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaS
 }
 
 template <int METHOD, bool HALF_TMP, typename HistT>
-static cudaError_t launch_blocks_t(const BatchStepDesc* desc, int* counter, int depth, int grid, cudaStream_t s) {
-    k_batch_blocks<METHOD, HALF_TMP, HistT><<<grid, kLocal, 0, s>>>(desc, counter, depth);
+static cudaError_t launch_blocks_t(const BatchStepDesc* desc, int* counter, int depth, int grid, bool pixels,
+                                   cudaStream_t s) {
+    if (pixels) k_batch_blocks<METHOD, HALF_TMP, HistT, true><<<grid, kLocal, 0, s>>>(desc, counter, depth);
+    else k_batch_blocks<METHOD, HALF_TMP, HistT, false><<<grid, kLocal, 0, s>>>(desc, counter, depth);
     return cudaGetLastError();
 }
 
 template <int METHOD, bool HALF_TMP, typename HistT>
 static int occupancy_t() {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<METHOD, HALF_TMP, HistT>, kLocal, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_blocks<METHOD, HALF_TMP, HistT, true>, kLocal,
+                                                  0);
     return per_sm;
 }
 
@@ -160,9 +186,10 @@ struct LaunchBlocks {
     const BatchStepDesc* desc;
     int* counter;
     int depth, grid;
+    bool pixels;
     cudaStream_t s;
     template <int M, bool H, typename T>
-    cudaError_t run() const { return launch_blocks_t<M, H, T>(desc, counter, depth, grid, s); }
+    cudaError_t run() const { return launch_blocks_t<M, H, T>(desc, counter, depth, grid, pixels, s); }
 };
 
 struct Occupancy {
@@ -171,8 +198,8 @@ struct Occupancy {
 };
 
 cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, int qr, bool half_tmp,
-                                bool half_history, int depth, int grid, cudaStream_t s) {
-    const LaunchBlocks l{desc, counter, depth, grid, s};
+                                bool half_history, int depth, int grid, bool pixels, cudaStream_t s) {
+    const LaunchBlocks l{desc, counter, depth, grid, pixels, s};
     if (half_history) return dispatch_blocks<__half>(qr, half_tmp, l);
     return dispatch_blocks<float>(qr, half_tmp, l);
 }
@@ -188,6 +215,13 @@ static cudaError_t launch_taa_t(const BatchStepDesc* desc, bool half_history, in
     const int grid = sms * 16;
     if (half_history) k_batch_taa<R, __half><<<grid, 128, 0, s>>>(desc);
     else k_batch_taa<R, float><<<grid, 128, 0, s>>>(desc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_wsacc_taa(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
+    const int grid = sms * 8;
+    if (half_history) k_batch_wsacc_taa<__half><<<grid, 256, 0, s>>>(desc);
+    else k_batch_wsacc_taa<float><<<grid, 256, 0, s>>>(desc);
     return cudaGetLastError();
 }
 

@@ -32,6 +32,7 @@ struct BatchTuning {
     int block_ctas_per_sm;   // persistent CTAs of the block kernel per SM
     int tile_w, tile_h;      // TAA CTA shape
     int staging_depth;       // blocks ahead whose inputs are prefetched into L2
+    int pixel_pass;          // 1: weighted sum + filtered accumulation + TAA over image tiles
 };
 
 // The step's kernels read everything from `desc` (device memory), so one
@@ -39,8 +40,11 @@ struct BatchTuning {
 cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaStream_t s);
 // grid: persistent CTAs (from batch_block_occupancy and the tuning).
 // qr: bmfr_params.fp32_qr (FitMethod).
+// pixels: the block kernel also runs weighted sum + filtered accumulation.
 cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, int qr, bool half_tmp,
-                                bool half_history, int depth, int grid, cudaStream_t s);
+                                bool half_history, int depth, int grid, bool pixels, cudaStream_t s);
+// The pixel pass: every stream's kWtTileW x kWtTileH image tiles.
+cudaError_t launch_batch_wsacc_taa(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s);
 cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const BatchTuning& t, int sms,
                              cudaStream_t s);
 int batch_block_occupancy(int qr, bool half_tmp, bool half_history);

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "batch.cuh"
+#include "pixel_ops.cuh"
 #include "bmfr_batch.h"
 #include "status.h"
 
@@ -104,7 +105,7 @@ struct bmfr_batch {
     int sms = 0;
     size_t budget = 0, used = 0;
     std::vector<StreamSlot> slots = std::vector<StreamSlot>(BMFR_BATCH_MAX_STREAMS);
-    bmfr::BatchTuning tuning{0, 30, 32, 0};
+    bmfr::BatchTuning tuning{0, 30, 32, 0, 0};
     int block_occupancy = 1;
     bmfr::BatchStepDesc* d_desc = nullptr;
     bmfr::BatchStepDesc* h_desc[2] = {nullptr, nullptr};
@@ -183,10 +184,14 @@ int build_graphs(bmfr_batch* b) {
         e = cudaMemcpyAsync(b->d_desc, b->h_desc[k], sizeof(bmfr::BatchStepDesc), cudaMemcpyHostToDevice, cs);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(int), cs);
         if (e == cudaSuccess) e = bmfr::launch_batch_noise(b->d_desc, BMFR_BATCH_MAX_STREAMS, cs);
+        const bool pixel_pass = b->tuning.pixel_pass != 0;
         if (e == cudaSuccess)
             e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr, half_tmp,
-                                          b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms, cs);
-        if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
+                                          b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms,
+                                          !pixel_pass, cs);
+        if (e == cudaSuccess)
+            e = pixel_pass ? bmfr::launch_batch_wsacc_taa(b->d_desc, b->p.half_history != 0, b->sms, cs)
+                           : bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[k], graph, 0);
@@ -217,7 +222,11 @@ bmfr::AccumArgs step_args(const bmfr_batch* b, const float* m, const float* off,
 // Fills description buffer k for the listed streams.
 int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, const bmfr_frame_io* io,
               const float* matrices, const float* offsets) {
-    const int tw = b->tuning.tile_w, th = b->tuning.tile_h;
+    // Image tiles of the step's per-pixel launch: TAA strips, or the pixel
+    // pass's tiles.
+    const bool pixel_pass = b->tuning.pixel_pass != 0;
+    const int tw = pixel_pass ? bmfr::kWtTileW : b->tuning.tile_w;
+    const int th = pixel_pass ? bmfr::kWtTileH : b->tuning.tile_h;
     int blocks = 0, tiles = 0;
     for (int i = 0; i < n; ++i) {
         StreamSlot& s = b->slots[slots[i]];
@@ -276,7 +285,7 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
 
 // The staged step on the streams of description d (host copy): for each
 // stream the plan's kernels — noise table, accumulation, fitter, weighted sum
-// + filtered accumulation, TAA — with the stream's buffers, the same
+// + filtered accumulation + TAA — with the stream's buffers, the same
 // launches and arithmetic as a plan's frame, so each stream's output equals
 // the plan's.  The streams are spread over the worker CUDA streams, largest
 // first onto the least loaded worker, forked from and joined into `s`.
@@ -315,13 +324,10 @@ cudaError_t launch_staged_step(bmfr_batch* b, const bmfr::BatchStepDesc& d, cuda
             e = bmfr::launch_fitter(g, f, J.job.nc, J.tmp, half_tmp, b->p.fp32_qr, fb.weights, fb.mins_maxs,
                                     fb.noise, b->d_status, ws);
         if (e == cudaSuccess)
-            e = bmfr::launch_weighted_sum_accumulate(g, f, J.job.second_alpha, fb.weights, fb.mins_maxs, fb.cur_n,
-                                                     fb.cur_p, nullptr, fb.prev_pix, fb.accept, fb.albedo,
-                                                     fb.tone_mapped, fb.cur_spp, fb.acc_prev, fb.acc_cur, half_hist,
-                                                     ws);
-        if (e == cudaSuccess)
-            e = bmfr::launch_taa(g, f, J.taa_alpha, fb.prev_pix, fb.tone_mapped, J.result_hist, J.result_prev,
-                                 J.result_out, half_hist, ws);
+            e = bmfr::launch_wsacc_taa(g, f, J.job.second_alpha, J.taa_alpha, fb.weights, fb.mins_maxs, fb.cur_n,
+                                       fb.cur_p, fb.prev_pix, fb.accept, fb.albedo, fb.cur_spp, fb.acc_prev,
+                                       fb.acc_cur, nullptr, nullptr, J.result_hist, J.result_prev, J.result_out,
+                                       half_hist, ws);
     }
     for (int w = 0; w < kStepWorkers && e == cudaSuccess; ++w) {
         if (!used[w]) continue;
@@ -708,6 +714,7 @@ int bmfr_batch_get_tuning(const bmfr_batch* b, bmfr_batch_tuning* t) {
     t->taa_tile_w = b->tuning.tile_w;
     t->taa_tile_h = b->tuning.tile_h;
     t->staging_depth = b->tuning.staging_depth;
+    t->pixel_pass = b->tuning.pixel_pass;
     return BMFR_OK;
 }
 
@@ -718,10 +725,12 @@ int bmfr_batch_set_tuning(bmfr_batch* b, const bmfr_batch_tuning* t) {
     if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 30x16, 30x32 or 30x64");
     if (t->block_ctas_per_sm < 0 || t->staging_depth < 0 || t->staging_depth > 4)
         return fail(BMFR_E_INVALID, "bad block CTAs per SM or staging depth");
+    if (t->pixel_pass != 0 && t->pixel_pass != 1) return fail(BMFR_E_INVALID, "pixel_pass must be 0 or 1");
     b->tuning.block_ctas_per_sm = t->block_ctas_per_sm;
     b->tuning.tile_w = t->taa_tile_w;
     b->tuning.tile_h = t->taa_tile_h;
     b->tuning.staging_depth = t->staging_depth;
+    b->tuning.pixel_pass = t->pixel_pass;
     return b->p.pipeline == BMFR_PIPELINE_STAGED ? BMFR_OK : build_graphs(b);   // the staged step has no graph
 }
 
@@ -746,7 +755,7 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
         *ms /= steps;
         return BMFR_OK;
     };
-    bmfr_batch_tuning best{0, 30, 32, 0};
+    bmfr_batch_tuning best{0, 30, 32, 0, 0};
     float best_t = 1e30f;
     int status = BMFR_OK;
     if (b->p.pipeline == BMFR_PIPELINE_STAGED) {
@@ -764,7 +773,7 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
     for (int ctas = 1; ctas <= b->block_occupancy && status == BMFR_OK; ++ctas) {
         const int max_depth = b->p.pipeline == BMFR_PIPELINE_STAGED ? 0 : 2;   // staging: fused step only
         for (int depth = 0; depth <= max_depth && status == BMFR_OK; ++depth) {
-            bmfr_batch_tuning t{ctas, 30, 32, depth};
+            bmfr_batch_tuning t{ctas, 30, 32, depth, 0};
             float ms = 0.f;
             status = time_tuning(t, &ms);
             if (status == BMFR_OK && ms < best_t) {
@@ -778,6 +787,17 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
         bmfr_batch_tuning t = best;
         t.taa_tile_w = shapes[i][0];
         t.taa_tile_h = shapes[i][1];
+        float ms = 0.f;
+        status = time_tuning(t, &ms);
+        if (status == BMFR_OK && ms < best_t) {
+            best_t = ms;
+            best = t;
+        }
+    }
+    // Then the per-pixel stages as their own pass over image tiles.
+    if (status == BMFR_OK) {
+        bmfr_batch_tuning t = best;
+        t.pixel_pass = 1;
         float ms = 0.f;
         status = time_tuning(t, &ms);
         if (status == BMFR_OK && ms < best_t) {

@@ -77,15 +77,16 @@ __device__ __forceinline__ float rop(float a, float b) {
 }
 
 // Batched work-group reduction of n <= VMAX values per thread.  Values
-// [0, split) use OP_A, [split, n) use OP_B (0 sum, 1 min, 2 max).
-template <int VMAX, int OP_A, int OP_B>
+// [0, split) use OP_A, [split, n) use OP_B (0 sum, 1 min, 2 max).  NMIN is a
+// compile-time lower bound on n: the guards of the values below it vanish.
+template <int VMAX, int OP_A, int OP_B, int NMIN = 0>
 __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int split, FitterSmem& sm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (OP_A == 0 && OP_B == 0) {
         // Sums, two values per packed add (bmfr.cl:33).
 #pragma unroll
         for (int i = 0; i < VMAX; i += 2) {
-            if (i < n) {
+            if (i < NMIN || i < n) {
                 const float a0 = v[i], a1 = i + 1 < VMAX ? v[i + 1] : 0.0f;
                 const float2 a = make_float2(a0, a1);
                 const float2 b = make_float2(__shfl_down_sync(kFull, a0, 8), __shfl_down_sync(kFull, a1, 8));
@@ -94,14 +95,14 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
                 const float2 s1 = __fadd2_rn(a, __fadd2_rn(__fadd2_rn(b, c), d));
                 if (lane < 8) {
                     sm.part[i * 64 + 8 * warp + lane] = s1.x;
-                    if (i + 1 < n) sm.part[(i + 1) * 64 + 8 * warp + lane] = s1.y;
+                    if (i + 1 < NMIN || i + 1 < n) sm.part[(i + 1) * 64 + 8 * warp + lane] = s1.y;
                 }
             }
         }
     } else {
 #pragma unroll
         for (int i = 0; i < VMAX; ++i) {
-            if (i < n) {
+            if (i < NMIN || i < n) {
                 const float a = v[i];
                 const float b = __shfl_down_sync(kFull, a, 8);
                 const float c = __shfl_down_sync(kFull, a, 16);
@@ -287,8 +288,9 @@ __device__ __forceinline__ void load_column(const Tile<HALF>& t, int k, int fb, 
 // are tile columns 1..V.  NOISE: the first column, whose dot products read
 // features 1..9 with noise added (bmfr.cl:625-627).
 // VS: column slots the loops visit (a compile-time bound >= the V later
-// columns): the late columns take a shorter instance.
-template <bool HALF, bool NOISE, int VS = 12>
+// columns): the late columns take a shorter instance.  VMIN: a compile-time
+// bound <= V, so that the slots below it are visited without a guard.
+template <bool HALF, bool NOISE, int VS = 12, int VMIN = 0>
 __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const float* __restrict__ noise,
                                           NoiseConst nc, FitterSmem& sm) {
     const int V = kBuffers - 1 - col;
@@ -325,7 +327,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
 #pragma unroll
     for (int i = 0; i < VS; i += 2) {
         d[i] = d[i + 1] = 0.0f;
-        if (i < V) {
+        if (i < VMIN || i < V) {
             float2 a01, a23, b01, b23;
             load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
             load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
@@ -337,7 +339,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             d[i + 1] = s.y;
         }
     }
-    block_reduce<VS, 0, 0>(d, V, V, sm);
+    block_reduce<VS, 0, 0, VMIN>(d, V, V, sm);
 
     // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
     // Quotients take Markstein's correction when every operand is in range:
@@ -356,7 +358,7 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     const float2 ny = dup2(-y), b2 = dup2(uls);
 #pragma unroll
     for (int i = 0; i < VS; ++i) {
-        if (i < V) {
+        if (i < VMIN || i < V) {
             const float dot = sm.out[i];
             const float ad = fabsf(dot);
             const bool fast = fast_u && (ad == 0.0f || (ad >= 0x1p-32f && ad <= 0x1p30f));
@@ -832,9 +834,9 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
         }
         qr_column<HALF, true>(t, 0, id, noise, nc, sm);
 #pragma unroll 1
-        for (int col = 1; col < 6; ++col) qr_column<HALF, false>(t, col, id, noise, nc, sm);        // 11..7 later columns
+        for (int col = 1; col < 6; ++col) qr_column<HALF, false, 12, 7>(t, col, id, noise, nc, sm);   // 11..7 later columns
 #pragma unroll 1
-        for (int col = 6; col < kFeatures; ++col) qr_column<HALF, false, 6>(t, col, id, noise, nc, sm);   // 6..3
+        for (int col = 6; col < kFeatures; ++col) qr_column<HALF, false, 6, 3>(t, col, id, noise, nc, sm);   // 6..3
     }
 
     // After ten shifts the colour columns are tile columns 0..2: rows 0..9

@@ -27,9 +27,12 @@ __device__ __forceinline__ void tile_set1(Tile<false>& t, int k, int q, float v)
 // kFitReference and HALF_TMP the tile is binary16, rounded at every store as
 // the reference rounds; HALF_TMP: features are rounded to binary16 as the
 // reference's tmp_data stores them (bmfr.cl:471-475); HistT: element type of
-// the colour histories.  Block b of job j; ends with every thread past the
+// the colour histories.  PIXELS: phase 3 (weighted sum and filtered
+// accumulation of the block's in-image pixels) runs here; without it the
+// block ends at the fit and a pass over image tiles runs them with TAA
+// (wsacc_taa_tile).  Block b of job j; ends with every thread past the
 // fit's final barrier.
-template <int METHOD, bool HALF_TMP, typename HistT>
+template <int METHOD, bool HALF_TMP, typename HistT, bool PIXELS = true>
 __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, FitterSmem& sm, float* w_s,
                                                  float* mm_s) {
     constexpr bool ROUND = HALF_TMP && METHOD == kFitReference;
@@ -101,6 +104,7 @@ __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, Fitte
     if (threadIdx.x < kFeatures * 3) fb.weights[(size_t)b * kFeatures * 3 + threadIdx.x] = w_s[threadIdx.x];
     if (threadIdx.x < kScaled * 2) fb.mins_maxs[(size_t)b * kScaled * 2 + threadIdx.x] = mm_s[threadIdx.x];
 
+    if constexpr (!PIXELS) return;
     // Phase 3: weighted_sum and accumulate_filtered_data of the owned pixels.
 #pragma unroll
     for (int q = 0; q < 4; ++q) {

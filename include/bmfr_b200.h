@@ -278,7 +278,10 @@ int bmfr_plan_reset(bmfr_plan* plan);   /* frame counter back to 0 */
 
 /* Intermediate buffers of the last frame, for inspection and tests.  Which
  * pointers exist depends on the pipeline: the fused pipeline keeps no
- * tmp_data or filtered frame (NULL). */
+ * tmp_data or filtered frame (NULL); the staged pipeline runs weighted_sum,
+ * accumulate_filtered_data and taa as one kernel, so its filtered and
+ * tone-mapped frames are written (non-NULL here) only while
+ * bmfr_plan_keep_intermediates is on. */
 typedef struct bmfr_plan_buffers {
     const void* tmp_data;
     const float* weights, *mins_maxs;
@@ -288,14 +291,19 @@ typedef struct bmfr_plan_buffers {
     const float* result;
 } bmfr_plan_buffers;
 int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
+/* Staged pipeline: enable (1) or disable (0, the default) writing the
+ * filtered and tone-mapped frames of every frame, which the reference keeps
+ * in global buffers (bmfr.cpp:331-340) and the plan otherwise keeps on chip.
+ * Outputs are the same either way. */
+int bmfr_plan_keep_intermediates(bmfr_plan* plan, int enable);
 
 /* Per-stage timing of the plan pipeline, in place of the reference's
  * per-kernel OpenCL event profiling (bmfr.cpp:386-412, 488-517).  While
  * enabled, every denoise call records CUDA events between its stages.
  * bmfr_plan_stage_times waits for the last frame and returns milliseconds of
  * the staged pipeline's [accumulate_noisy_data (with the frame's fitter
- * noise table), fitter, weighted_sum + accumulate_filtered_data (one kernel
- * in the plan pipeline), 0, taa].  The fused pipeline reports [noise table,
+ * noise table), fitter, weighted_sum + accumulate_filtered_data + taa (one
+ * kernel in the plan pipeline), 0, 0].  The fused pipeline reports [noise table,
  * block kernel (accumulate, fitter, weighted sum and filtered accumulation),
  * 0, 0, taa].  The five drop-in stage entry points time separately with
  * events around each call. */

@@ -52,6 +52,11 @@ typedef struct bmfr_batch_tuning {
                                order with the inputs of each CTA's next k blocks prefetched
                                into L2.  The staged step launches a plan's kernels, whose
                                shapes are fixed: it has nothing to tune. */
+    int pixel_pass;         /* fused step: 0 runs weighted sum + filtered accumulation in the
+                               block kernel after each block's fit, then TAA over 30-column
+                               strips; 1 ends the block kernel at the fit and runs weighted
+                               sum + filtered accumulation + TAA as one pass over 32x8 image
+                               tiles (the taa_tile fields are then unused) */
 } bmfr_batch_tuning;
 
 /* memory_budget_bytes: device bytes the batch's streams may hold (0: no limit).

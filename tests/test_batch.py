@@ -118,6 +118,35 @@ def test_staged_step_with_more_streams_than_workers(cuda):
 
 
 @pytest.mark.parametrize("qr", [B.QR_REFERENCE, B.QR_CHOLESKY2])
+def test_fused_step_with_the_pixel_pass(cuda, qr):
+    """The fused step with its per-pixel stages as a pass over image tiles
+    (the block kernel ends at the fit): every stream still equals its
+    plan's output bit for bit, over steps of all streams and of a subset."""
+    import torch
+    kw = dict(fp32_qr=qr, half_history=1) if qr != B.QR_REFERENCE else {}
+    params = B.default_params(pipeline=B.PIPELINE_FUSED, **kw)
+    streams = [Stream(50 + k, w, h, params, cuda) for k, (w, h) in enumerate(SIZES)]
+    batch = B.Batch(params)
+    batch.set_tuning(pixel_pass=1)
+    assert batch.tuning.pixel_pass == 1
+    slots = [batch.add_stream(s.w, s.h) for s in streams]
+    frame = [0] * len(streams)
+    for active in ([0, 1, 2, 3], [2, 0], [0, 1, 2, 3]):
+        io = [streams[i].io(frame[i]) for i in active]
+        mats = np.concatenate([streams[i].sc.prev_camera(frame[i]) for i in active])
+        offs = np.concatenate([streams[i].sc.pixel_offset(frame[i]) for i in active])
+        batch.step([slots[i] for i in active], mats, offs, io=io)
+        for i in active:
+            s = streams[i]
+            want = s.plan_step(frame[i]).cpu().numpy().reshape(s.h, s.w, 3)
+            np.testing.assert_array_equal(_device_result(batch.result_ptr(slots[i]), s.w, s.h), want,
+                                          err_msg=f"stream {i} frame {frame[i]}")
+            frame[i] += 1
+    torch.cuda.synchronize()
+    batch.close()
+
+
+@pytest.mark.parametrize("qr", [B.QR_REFERENCE, B.QR_CHOLESKY2])
 def test_fused_step_queue_longer_than_the_grid(cuda, qr):
     """Two 640x360 streams: 572 blocks in the fused step's queue, more than
     its persistent CTAs, so CTAs take several blocks each; every result

@@ -50,6 +50,7 @@ def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     sc = B.Scene(21, W, H, 12)
     plan = B.Plan(W, H, pipeline=pipeline, position_limit_squared=sc.position_limit_squared,
                   normal_limit_squared=sc.normal_limit_squared)
+    plan.keep_intermediates(True)   # the tone-mapped frame is checked below
     ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared))
     for f in range(frames):
         d = sc.render(f)
@@ -75,6 +76,47 @@ def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     torch.cuda.synchronize()
     assert plan.frame_number == frames
     plan.close()
+
+
+@pytest.mark.parametrize("half_history", [0, 1])
+def test_kept_intermediates_change_no_output(cuda, half_history):
+    """The staged pipeline runs weighted sum, filtered accumulation and TAA as
+    one kernel; writing its filtered and tone-mapped frames out for
+    inspection must not change any output bit, and those frames must equal
+    the drop-in entry points' on the same frame."""
+    import torch
+    W, H = 200, 120
+    sc = B.Scene(24, W, H, 12)
+    kw = dict(half_history=half_history, fp32_qr=1 if half_history else 0,
+              position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
+    plain, kept = B.Plan(W, H, **kw), B.Plan(W, H, **kw)
+    kept.keep_intermediates(True)
+    assert plain.buffers().tone_mapped is None and plain.buffers().filtered is None
+    for f in range(4):
+        d = sc.render(f)
+        for pl in (plain, kept):
+            pl.upload_frame(d["albedo"], d["normals"], d["positions"], d["noisy"])
+            pl.denoise_frame(sc.prev_camera(f), sc.pixel_offset(f))
+        np.testing.assert_array_equal(plain.download_result(), kept.download_result(), err_msg=f"frame {f}")
+        hist = np.float16 if half_history else np.float32
+        a, b = plain.buffers(), kept.buffers()
+        np.testing.assert_array_equal(device_array(a.accumulated_filtered, (H, W, 3), hist),
+                                      device_array(b.accumulated_filtered, (H, W, 3), hist))
+        # The kept frames are the drop-in weighted_sum's and
+        # accumulate_filtered_data's outputs (float histories only: the
+        # drop-in entry points take float buffers).
+        if not half_history and f > 0:
+            n = W * H * 3
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).reshape(-1).to(cuda)
+            ptr = lambda p, shape, dt: torch.from_numpy(device_array(p, shape, dt)).reshape(-1).to(cuda)
+            filt = torch.empty(n, dtype=torch.float32, device=cuda)
+            B.weighted_sum(kept, ptr(b.weights, (kept.sizes.blocks * 30,), np.float32),
+                           ptr(b.mins_maxs, (kept.sizes.blocks * 12,), np.float32), filt, t(d["normals"]),
+                           t(d["positions"]), None, f)
+            np.testing.assert_array_equal(filt.cpu().numpy().reshape(H, W, 3),
+                                          device_array(b.filtered, (H, W, 3), np.float32))
+    plain.close()
+    kept.close()
 
 
 def test_pipeline_rejects_bad_arguments(cuda):
