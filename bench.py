@@ -636,6 +636,37 @@ def measure_served(args, world, rank, local, dev, barrier, seconds):
     cap_same = capacity_of_plans(dict(fp32_qr=params.fp32_qr, half_history=params.half_history,
                                       pipeline=params.pipeline))
 
+    # ---- the server saturated: every capacity stream's next frames queued at
+    # once, so that each step takes a frame of every stream -------------------
+    sat_frames = 8
+    sat = B.Server(params)
+    sat.set_tuning(tuning)
+    sat_ids = [sat.open_stream(pools[st["cls"]]["w"], pools[st["cls"]]["h"]) for st in cap_streams]
+    for i in range(2):   # warm-up frames
+        for st, sid in zip(cap_streams, sat_ids):
+            io, m, o = pools[st["cls"]]["tab"][(st["phase"] + i) % period][:3]
+            sat.submit(sid, m, o, io=io)
+    sat.drain(120000)
+    sat.reset_stats()
+    ts = time.perf_counter()
+    for i in range(2, 2 + sat_frames):
+        for st, sid in zip(cap_streams, sat_ids):
+            io, m, o = pools[st["cls"]]["tab"][(st["phase"] + i) % period][:3]
+            sat.submit(sid, m, o, io=io)
+    sat.drain(120000)
+    sat_s = time.perf_counter() - ts
+    sst = sat.stats()
+    for sid in sat_ids:
+        sat.close_stream(sid)
+    sat.close()
+    torch.cuda.synchronize()
+    saturated = {"value": len(cap_streams) * sat_frames / sat_s, "unit": "frames/s",
+                 "frames_per_step": sst["mean_frames_per_step"], "steps": int(sst["steps"]),
+                 "latency_ms": {"p50": sst["p50_latency_ms"], "p99": sst["p99_latency_ms"]},
+                 "how": f"{len(cap_streams)} streams, {sat_frames} frames each submitted at once through the "
+                        f"server (wall clock from the first submit to the drain); latency here is mostly "
+                        f"queueing"}
+
     # Peak stream memory and peak open streams per class over the trace:
     # both paths reserve them before the trace starts.
     live, peak_bytes, per_cls, peak_cls = 0, 0, [0] * len(SERVED_MIX), [0] * len(SERVED_MIX)
@@ -841,6 +872,7 @@ def measure_served(args, world, rank, local, dev, barrier, seconds):
                            "frames_before_admission": plain_not_admitted[0],
                            "how": "one staged plan per stream (reference arithmetic, float histories), "
                                   "requests in arrival order on one CUDA stream, plans reused across streams"},
+            "saturated_server": saturated,
             "capacity": {"batched": cap_batched, "plain": cap_plain, "ratio": cap_batched / cap_plain,
                          "same_arithmetic_plans": cap_same, "ratio_vs_same_arithmetic": cap_batched / cap_same,
                          "unit": "frames/s", "streams": len(cap_streams),
