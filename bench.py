@@ -91,10 +91,10 @@ def stage_bytes(w, h):
         # tone-mapped frame stays on chip
         "weighted_sum+accumulate_filtered_data+taa": 94 * P,
         "noise_table": 9 * 4 * 256 * 4,
-        # accumulate (95 B/px + 26 B read per margin pixel from the inputs, no
-        # tmp_data) + weighted sum and filtered accumulation (82 B/px less the
-        # 24 B/px of N, P re-read from L2) -> counted once per byte of HBM.
-        "block_kernel": 95 * P + 24 * (Pm - P) + 168 * B + 58 * P,
+        # accumulate (95 B/px, and the margin-only pixels' 24 B of N, P read
+        # again from their mirror) and the fit's weights and min/max; no
+        # tmp_data
+        "block_kernel": 95 * P + 24 * (Pm - P) + 168 * B,
     }
 
 
@@ -469,9 +469,10 @@ def measure_batched(args, world, rank, local, dev, barrier, steps, warmup):
         "speedup_vs_plain": value / plain_value / world,
         "speedup_vs_same_arithmetic_plans": value / prec_value / world,
         "clocks": clocks.summary(),
-        # per step: noise table, block kernel, TAA (fused); per stream noise
-        # table, accumulation, fitter, weighted sum + filtered accumulation, TAA (staged)
-        "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 5 * n) * steps * len(loop_ms),
+        # per step: noise table, block kernel, image-tile kernel (fused); per
+        # stream noise table, accumulation, fitter, weighted sum + filtered
+        # accumulation + TAA (staged)
+        "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 4 * n) * steps * len(loop_ms),
     }
 
 
@@ -880,9 +881,9 @@ def measure_served(args, world, rank, local, dev, barrier, seconds):
                                 "step per frame of all streams (staged: each stream's plan kernels on eight "
                                 "worker CUDA streams; fused: one graph-captured block-queue launch); plain: "
                                 "their plans in turn"},
-            # per step: 5 kernels per listed stream (staged) or noise, block kernel, TAA (fused)
+            # per step: 4 kernels per listed stream (staged) or noise, block kernel, image tiles (fused)
             "clocks": clocks.summary(),
-            "gpu_launches": (5 * int(st.get("frames", 0)) if args.pipeline == "staged" else 3 * int(st["steps"])),
+            "gpu_launches": (4 * int(st.get("frames", 0)) if args.pipeline == "staged" else 3 * int(st["steps"])),
         }
 
 
@@ -1216,9 +1217,10 @@ def main():
     barrier()
     elapsed_ms = max_over_ranks(statistics.median(loop_ms), device=dev)   # the slowest rank
     value = world * args.steps / (elapsed_ms / 1e3)
-    # noise table, block kernel, taa (fused); noise table, accumulate, fitter,
-    # weighted sum + filtered accumulation, taa (staged)
-    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 5
+    # noise table, block kernel, weighted sum + filtered accumulation + taa
+    # (fused); noise table, accumulate, fitter, weighted sum + filtered
+    # accumulation + taa (staged)
+    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 4
 
     # ---- per-stage profile (same workload, events between stages) ------------
     plan.enable_profiling(True)

@@ -63,7 +63,7 @@ struct bmfr_plan {
     const float* last_result = nullptr;         // float32 output of the last frame
     bool profiling = false;
     bool profiled_frame = false;
-    bool keep_intermediates = false;            // staged: also write filtered and tone-mapped frames
+    bool keep_intermediates = false;            // also write the filtered and tone-mapped frames
     cudaEvent_t events[6] = {};                 // stage boundaries of the last frame
     // Ordering of uploads, frames and downloads that run on different
     // streams: input set k uploaded, frame f done (index f % 3), result of
@@ -519,7 +519,7 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         fb.noise = plan->noise_table;
         if (e == cudaSuccess)
             e = bmfr::launch_fused_block(g, a, bmfr::make_noise_const(plan->p.noise_amount),
-                                         plan->p.second_blend_alpha, plan->p.fp32_qr, half_hist, fb, s);
+                                         plan->p.second_blend_alpha, plan->p.fp32_qr, half_hist, fb, false, s);
         mark(2);
     } else {
         if (e == cudaSuccess)
@@ -534,26 +534,18 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         mark(2);
     }
     float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
-    if (plan->p.pipeline == BMFR_PIPELINE_FUSED) {
-        mark(3);
-        mark(4);
-        if (e == cudaSuccess)
-            e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped,
-                                 plan->result[cur], plan->result[prv], f32_out, half_hist, s);
-    } else {
-        // weighted_sum, accumulate_filtered_data and taa in one kernel: the
-        // filtered and tone-mapped frames stay on chip unless kept for
-        // inspection (bmfr_plan_keep_intermediates).
-        const bool keep = plan->keep_intermediates;
-        if (e == cudaSuccess)
-            e = bmfr::launch_wsacc_taa(g, f, plan->p.second_blend_alpha, plan->p.taa_blend_alpha, plan->weights,
-                                       plan->mins_maxs, cur_n, cur_p, plan->prev_pix, plan->accept, albedo,
-                                       plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur],
-                                       keep ? plan->filtered : nullptr, keep ? plan->tone_mapped : nullptr,
-                                       plan->result[cur], plan->result[prv], f32_out, half_hist, s);
-        mark(3);
-        mark(4);
-    }
+    // Both pipelines end with weighted_sum, accumulate_filtered_data and taa
+    // in one kernel: the filtered and tone-mapped frames stay on chip unless
+    // kept for inspection (bmfr_plan_keep_intermediates).
+    const bool keep = plan->keep_intermediates;
+    if (e == cudaSuccess)
+        e = bmfr::launch_wsacc_taa(g, f, plan->p.second_blend_alpha, plan->p.taa_blend_alpha, plan->weights,
+                                   plan->mins_maxs, cur_n, cur_p, plan->prev_pix, plan->accept, albedo,
+                                   plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur],
+                                   keep ? plan->filtered : nullptr, keep ? plan->tone_mapped : nullptr,
+                                   plan->result[cur], plan->result[prv], f32_out, half_hist, s);
+    mark(3);
+    mark(4);
     mark(5);
     if (e == cudaSuccess) e = cudaEventRecord(plan->ev_frame_done[f % 3], s);
     if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
@@ -677,12 +669,12 @@ int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* b) {
     std::memset(b, 0, sizeof *b);
     const int last = (plan->frame + 1) & 1;   // slot written by the last frame
     const bool staged = plan->p.pipeline == BMFR_PIPELINE_STAGED;
-    b->tmp_data = plan->tmp;
+    b->tmp_data = staged ? plan->tmp : nullptr;   // the fused pipeline keeps tmp_data on chip
     b->weights = plan->weights;
     b->mins_maxs = plan->mins_maxs;
-    b->filtered = staged && plan->keep_intermediates ? plan->filtered : nullptr;
+    b->filtered = plan->keep_intermediates ? plan->filtered : nullptr;
     b->prev_frame_pixel = reinterpret_cast<const float*>(plan->prev_pix);
-    b->tone_mapped = !staged || plan->keep_intermediates ? plan->tone_mapped : nullptr;
+    b->tone_mapped = plan->keep_intermediates ? plan->tone_mapped : nullptr;
     b->accept = plan->accept;
     b->spp = plan->spp[last];
     b->accumulated_noisy = plan->noisy_acc[last];

@@ -117,8 +117,10 @@ struct BlockJob {
     FusedBuffers fb;
 };
 
+// pixels: the block kernel also runs weighted sum + filtered accumulation of
+// the block's in-image pixels (tone-mapped frame written for a TAA launch).
 cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
-                               int qr, bool half_history, const FusedBuffers& fb, cudaStream_t s);
+                               int qr, bool half_history, const FusedBuffers& fb, bool pixels, cudaStream_t s);
 
 // NOISE_AMOUNT * 2 split into hi + lo floats.
 inline NoiseConst make_noise_const(double noise_amount) {

@@ -58,8 +58,10 @@ extern "C" {
 
 /* Pipeline variants of bmfr_denoise_frame / bmfr_batch_step. */
 #define BMFR_PIPELINE_STAGED 0  /* the five stage kernels, reference order   */
-#define BMFR_PIPELINE_FUSED 1   /* accumulate+fit+weighted sum+filtered in
-                                   one kernel per 32x32 block, then TAA      */
+#define BMFR_PIPELINE_FUSED 1   /* accumulate+fit in one kernel per 32x32
+                                   block (tmp_data stays on chip), then
+                                   weighted sum+filtered accumulation+TAA
+                                   in one kernel over image tiles            */
 
 /* Runtime form of the reference's compile-time options.  Defaults
  * (bmfr_params_default) are the reference's values.  */
@@ -278,10 +280,9 @@ int bmfr_plan_reset(bmfr_plan* plan);   /* frame counter back to 0 */
 
 /* Intermediate buffers of the last frame, for inspection and tests.  Which
  * pointers exist depends on the pipeline: the fused pipeline keeps no
- * tmp_data or filtered frame (NULL); the staged pipeline runs weighted_sum,
- * accumulate_filtered_data and taa as one kernel, so its filtered and
- * tone-mapped frames are written (non-NULL here) only while
- * bmfr_plan_keep_intermediates is on. */
+ * tmp_data (NULL); both pipelines run weighted_sum, accumulate_filtered_data
+ * and taa as one kernel, so the filtered and tone-mapped frames are written
+ * (non-NULL here) only while bmfr_plan_keep_intermediates is on. */
 typedef struct bmfr_plan_buffers {
     const void* tmp_data;
     const float* weights, *mins_maxs;
@@ -291,10 +292,10 @@ typedef struct bmfr_plan_buffers {
     const float* result;
 } bmfr_plan_buffers;
 int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
-/* Staged pipeline: enable (1) or disable (0, the default) writing the
- * filtered and tone-mapped frames of every frame, which the reference keeps
- * in global buffers (bmfr.cpp:331-340) and the plan otherwise keeps on chip.
- * Outputs are the same either way. */
+/* Enable (1) or disable (0, the default) writing the filtered and
+ * tone-mapped frames of every frame, which the reference keeps in global
+ * buffers (bmfr.cpp:331-340) and the plan otherwise keeps on chip.  Outputs
+ * are the same either way. */
 int bmfr_plan_keep_intermediates(bmfr_plan* plan, int enable);
 
 /* Per-stage timing of the plan pipeline, in place of the reference's
@@ -304,9 +305,9 @@ int bmfr_plan_keep_intermediates(bmfr_plan* plan, int enable);
  * the staged pipeline's [accumulate_noisy_data (with the frame's fitter
  * noise table), fitter, weighted_sum + accumulate_filtered_data + taa (one
  * kernel in the plan pipeline), 0, 0].  The fused pipeline reports [noise table,
- * block kernel (accumulate, fitter, weighted sum and filtered accumulation),
- * 0, 0, taa].  The five drop-in stage entry points time separately with
- * events around each call. */
+ * block kernel (accumulate and fitter), weighted_sum +
+ * accumulate_filtered_data + taa, 0, 0].  The five drop-in stage entry
+ * points time separately with events around each call. */
 #define BMFR_STAGE_COUNT 5
 int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable);
 int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);
