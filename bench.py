@@ -82,14 +82,11 @@ def stage_bytes(w, h):
         "fitter": 26 * Pm + 168 * B,
         "weighted_sum": 36 * P,
         "accumulate_filtered_data": 70 * P,
-        # one pass: N, P, prev_pix, accept, albedo, spp, acc_prev read; filtered,
-        # acc_cur, tone_mapped written (float histories)
-        "weighted_sum+accumulate_filtered_data": 94 * P,
+        # one pass: N, P, prev_pix, accept, albedo, spp, acc_prev read; acc_cur
+        # and tone_mapped written (float histories; the filtered colour stays
+        # on chip)
+        "weighted_sum+accumulate_filtered_data": 82 * P,
         "taa": 44 * P,
-        # one kernel: N, P, prev_pix, accept, albedo, spp, the filtered and
-        # TAA histories read; both histories written (float histories); the
-        # tone-mapped frame stays on chip
-        "weighted_sum+accumulate_filtered_data+taa": 94 * P,
         "noise_table": 9 * 4 * 256 * 4,
         # accumulate (95 B/px, and the margin-only pixels' 24 B of N, P read
         # again from their mirror) and the fit's weights and min/max; no
@@ -469,10 +466,11 @@ def measure_batched(args, world, rank, local, dev, barrier, steps, warmup):
         "speedup_vs_plain": value / plain_value / world,
         "speedup_vs_same_arithmetic_plans": value / prec_value / world,
         "clocks": clocks.summary(),
-        # per step: noise table, block kernel, image-tile kernel (fused); per
+        # per step: noise table, block kernel, (pixel pass,) TAA (fused); per
         # stream noise table, accumulation, fitter, weighted sum + filtered
-        # accumulation + TAA (staged)
-        "gpu_launches": (3 if pipeline == B.PIPELINE_FUSED else 4 * n) * steps * len(loop_ms),
+        # accumulation, TAA (staged)
+        "gpu_launches": (3 + tuning.pixel_pass if pipeline == B.PIPELINE_FUSED else 5 * n) * steps
+                        * len(loop_ms),
     }
 
 
@@ -881,9 +879,10 @@ def measure_served(args, world, rank, local, dev, barrier, seconds):
                                 "step per frame of all streams (staged: each stream's plan kernels on eight "
                                 "worker CUDA streams; fused: one graph-captured block-queue launch); plain: "
                                 "their plans in turn"},
-            # per step: 4 kernels per listed stream (staged) or noise, block kernel, image tiles (fused)
+            # per step: 5 kernels per listed stream (staged) or noise, block kernel, (pixel pass,) TAA (fused)
             "clocks": clocks.summary(),
-            "gpu_launches": (4 * int(st.get("frames", 0)) if args.pipeline == "staged" else 3 * int(st["steps"])),
+            "gpu_launches": (5 * int(st.get("frames", 0)) if args.pipeline == "staged"
+                             else (3 + tuning.pixel_pass) * int(st["steps"])),
         }
 
 
@@ -1217,10 +1216,10 @@ def main():
     barrier()
     elapsed_ms = max_over_ranks(statistics.median(loop_ms), device=dev)   # the slowest rank
     value = world * args.steps / (elapsed_ms / 1e3)
-    # noise table, block kernel, weighted sum + filtered accumulation + taa
+    # noise table, block kernel, weighted sum + filtered accumulation, taa
     # (fused); noise table, accumulate, fitter, weighted sum + filtered
-    # accumulation + taa (staged)
-    launches_per_frame = 3 if pipeline == B.PIPELINE_FUSED else 4
+    # accumulation, taa (staged)
+    launches_per_frame = 4 if pipeline == B.PIPELINE_FUSED else 5
 
     # ---- per-stage profile (same workload, events between stages) ------------
     plan.enable_profiling(True)

@@ -218,8 +218,8 @@ class Plan:
         check(lib.bmfr_plan_probe_bounded_wait(self.handle, int(limit_us), _stream_ptr(stream)),
               "bmfr_plan_probe_bounded_wait")
 
-    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data+taa", None, None)
-    FUSED_STAGES = ("noise_table", "block_kernel", "weighted_sum+accumulate_filtered_data+taa", None, None)
+    STAGES = ("accumulate_noisy_data", "fitter", "weighted_sum+accumulate_filtered_data", None, "taa")
+    FUSED_STAGES = ("noise_table", "block_kernel", "weighted_sum+accumulate_filtered_data", None, "taa")
 
     def stage_times(self) -> dict:
         """Milliseconds per kernel of the last profiled frame (the staged
@@ -230,8 +230,8 @@ class Plan:
         return {n: float(v) for n, v in zip(names, ms) if n is not None}
 
     def keep_intermediates(self, enable: bool = True) -> None:
-        """Also write the filtered and tone-mapped frames of every frame
-        (for inspection; outputs are unchanged)."""
+        """Also write the filtered frame of every frame (for inspection;
+        outputs are unchanged)."""
         check(lib.bmfr_plan_keep_intermediates(self.handle, int(enable)), "bmfr_plan_keep_intermediates")
 
     def buffers(self) -> PlanBuffers:

@@ -4,8 +4,8 @@
 // 32x32 blocks forming one global queue that a single persistent launch of
 // the fused block kernel walks (accumulate + fit, and with the pixel pass
 // off weighted sum + filtered accumulation, per block, fused_block.cuh),
-// then one launch over the streams' image tiles: TAA, or with the pixel
-// pass weighted sum + filtered accumulation + TAA (wsacc_taa_tile).  Both read the step's description from device memory,
+// with the pixel pass a launch over the streams' pixel tiles for weighted
+// sum + filtered accumulation, then one launch over their TAA tiles.  Both read the step's description from device memory,
 // so one captured CUDA graph serves every step.  (The staged step runs the
 // plan's kernels per stream, batch_host.cu.)
 #include <type_traits>
@@ -132,22 +132,33 @@ __global__ void __launch_bounds__(128) k_batch_taa(const BatchStepDesc* __restri
     }
 }
 
-// weighted_sum + accumulate_filtered_data + taa over every stream's image
-// tiles of kWtTileW x kWtTileH (the step's tiles with the pixel pass).
+__device__ __forceinline__ int stream_of_px_tile(const BatchStepDesc* __restrict__ d, int tile) {
+    int lo = 0, hi = d->n_streams - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (d->s[mid].px_tile_start <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The pixel pass: weighted_sum + accumulate_filtered_data over every
+// stream's 32x8 pixel tiles (one thread per pixel, as the plan's kernel),
+// the tone-mapped frame written for the TAA launch that follows.
 template <typename HistT>
-__global__ void __launch_bounds__(256, 4) k_batch_wsacc_taa(const BatchStepDesc* __restrict__ d) {
-    __shared__ float4 s_ycc[kWtRingPixels], s_rgb[kWtRingPixels];
-    const int nt = d->n_tiles;
+__global__ void __launch_bounds__(256) k_batch_wsacc(const BatchStepDesc* __restrict__ d) {
+    const int nt = d->n_px_tiles;
     for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-        const int s = stream_of_tile(d, tile);
+        const int s = stream_of_px_tile(d, tile);
         const BatchStreamJob& J = d->s[s];
         const FusedBuffers& fb = J.job.fb;
-        const int t = tile - J.tile_start;
-        wsacc_taa_tile<HistT>(J.job.g, J.job.a.frame, J.job.second_alpha, J.taa_alpha, fb.weights, fb.mins_maxs,
-                              fb.cur_n, fb.cur_p, fb.prev_pix, fb.accept, fb.albedo, fb.cur_spp,
-                              (const HistT*)fb.acc_prev, (HistT*)fb.acc_cur, nullptr, nullptr,
-                              (HistT*)J.result_hist, (const HistT*)J.result_prev, J.result_out,
-                              (t % J.tiles_x) * kWtTileW, (t / J.tiles_x) * kWtTileH, s_ycc, s_rgb);
+        const Geometry& g = J.job.g;
+        const int t = tile - J.px_tile_start;
+        const int px = (t % J.px_tiles_x) * 32 + (threadIdx.x & 31), py = (t / J.px_tiles_x) * 8 + (threadIdx.x >> 5);
+        if (px < g.W && py < g.H)
+            wsacc_px<HistT>(g, J.job.a.frame, J.job.second_alpha, px, py, fb.weights, fb.mins_maxs, fb.cur_n,
+                            fb.cur_p, nullptr, fb.prev_pix, fb.accept, fb.albedo, fb.tone_mapped, fb.cur_spp,
+                            (const HistT*)fb.acc_prev, (HistT*)fb.acc_cur);
     }
 }
 
@@ -218,10 +229,10 @@ static cudaError_t launch_taa_t(const BatchStepDesc* desc, bool half_history, in
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_wsacc_taa(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
-    const int grid = sms * 8;
-    if (half_history) k_batch_wsacc_taa<__half><<<grid, 256, 0, s>>>(desc);
-    else k_batch_wsacc_taa<float><<<grid, 256, 0, s>>>(desc);
+cudaError_t launch_batch_wsacc(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s) {
+    const int grid = sms * 32;
+    if (half_history) k_batch_wsacc<__half><<<grid, 256, 0, s>>>(desc);
+    else k_batch_wsacc<float><<<grid, 256, 0, s>>>(desc);
     return cudaGetLastError();
 }
 

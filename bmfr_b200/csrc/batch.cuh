@@ -16,6 +16,8 @@ struct BatchStreamJob {
     int block_start;           // first block of this stream in the step's block queue
     int tile_start;            // first TAA tile of this stream
     int tiles_x;               // TAA tiles per image row (for the step's tile shape)
+    int px_tile_start;         // first 32x8 pixel tile of this stream (the pixel pass)
+    int px_tiles_x;            // pixel tiles per image row
     float taa_alpha;
     void* result_hist;         // TAA history written this frame (float or binary16)
     const void* result_prev;   // TAA history of the previous frame
@@ -24,7 +26,7 @@ struct BatchStreamJob {
 };
 
 struct BatchStepDesc {
-    int n_streams, n_blocks, n_tiles, tile_w;
+    int n_streams, n_blocks, n_tiles, tile_w, n_px_tiles;
     BatchStreamJob s[kBatchMaxStreams];
 };
 
@@ -32,7 +34,7 @@ struct BatchTuning {
     int block_ctas_per_sm;   // persistent CTAs of the block kernel per SM
     int tile_w, tile_h;      // TAA CTA shape
     int staging_depth;       // blocks ahead whose inputs are prefetched into L2
-    int pixel_pass;          // 1: weighted sum + filtered accumulation + TAA over image tiles
+    int pixel_pass;          // 1: weighted sum + filtered accumulation as a pass over pixel tiles
 };
 
 // The step's kernels read everything from `desc` (device memory), so one
@@ -43,8 +45,9 @@ cudaError_t launch_batch_noise(const BatchStepDesc* desc, int max_streams, cudaS
 // pixels: the block kernel also runs weighted sum + filtered accumulation.
 cudaError_t launch_batch_blocks(const BatchStepDesc* desc, int* counter, int qr, bool half_tmp,
                                 bool half_history, int depth, int grid, bool pixels, cudaStream_t s);
-// The pixel pass: every stream's kWtTileW x kWtTileH image tiles.
-cudaError_t launch_batch_wsacc_taa(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s);
+// The pixel pass: weighted sum + filtered accumulation over every stream's
+// 32x8 pixel tiles, one thread per pixel.
+cudaError_t launch_batch_wsacc(const BatchStepDesc* desc, bool half_history, int sms, cudaStream_t s);
 cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const BatchTuning& t, int sms,
                              cudaStream_t s);
 int batch_block_occupancy(int qr, bool half_tmp, bool half_history);

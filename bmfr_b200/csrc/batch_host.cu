@@ -10,7 +10,6 @@
 #include <vector>
 
 #include "batch.cuh"
-#include "pixel_ops.cuh"
 #include "bmfr_batch.h"
 #include "status.h"
 
@@ -189,9 +188,8 @@ int build_graphs(bmfr_batch* b) {
             e = bmfr::launch_batch_blocks(b->d_desc, b->d_counters, b->p.fp32_qr, half_tmp,
                                           b->p.half_history != 0, b->tuning.staging_depth, ctas * b->sms,
                                           !pixel_pass, cs);
-        if (e == cudaSuccess)
-            e = pixel_pass ? bmfr::launch_batch_wsacc_taa(b->d_desc, b->p.half_history != 0, b->sms, cs)
-                           : bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
+        if (e == cudaSuccess && pixel_pass) e = bmfr::launch_batch_wsacc(b->d_desc, b->p.half_history != 0, b->sms, cs);
+        if (e == cudaSuccess) e = bmfr::launch_batch_taa(b->d_desc, b->p.half_history != 0, b->tuning, b->sms, cs);
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[k], graph, 0);
@@ -222,12 +220,8 @@ bmfr::AccumArgs step_args(const bmfr_batch* b, const float* m, const float* off,
 // Fills description buffer k for the listed streams.
 int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, const bmfr_frame_io* io,
               const float* matrices, const float* offsets) {
-    // Image tiles of the step's per-pixel launch: TAA strips, or the pixel
-    // pass's tiles.
-    const bool pixel_pass = b->tuning.pixel_pass != 0;
-    const int tw = pixel_pass ? bmfr::kWtTileW : b->tuning.tile_w;
-    const int th = pixel_pass ? bmfr::kWtTileH : b->tuning.tile_h;
-    int blocks = 0, tiles = 0;
+    const int tw = b->tuning.tile_w, th = b->tuning.tile_h;
+    int blocks = 0, tiles = 0, px_tiles = 0;
     for (int i = 0; i < n; ++i) {
         StreamSlot& s = b->slots[slots[i]];
         const int f = s.frame, cur = f & 1, prv = cur ^ 1;
@@ -268,6 +262,9 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
         J.block_start = blocks;
         J.tile_start = tiles;
         J.tiles_x = (s.width + tw - 1) / tw;
+        J.px_tile_start = px_tiles;
+        J.px_tiles_x = (s.width + 31) / 32;
+        px_tiles += J.px_tiles_x * ((s.height + 7) / 8);
         J.taa_alpha = b->p.taa_blend_alpha;
         J.result_hist = s.result[cur];
         J.result_prev = s.result[prv];
@@ -279,13 +276,14 @@ int fill_desc(bmfr_batch* b, bmfr::BatchStepDesc* d, int n, const int* slots, co
     d->n_streams = n;
     d->n_blocks = blocks;
     d->n_tiles = tiles;
+    d->n_px_tiles = px_tiles;
     d->tile_w = tw;
     return BMFR_OK;
 }
 
 // The staged step on the streams of description d (host copy): for each
 // stream the plan's kernels — noise table, accumulation, fitter, weighted sum
-// + filtered accumulation + TAA — with the stream's buffers, the same
+// + filtered accumulation, TAA — with the stream's buffers, the same
 // launches and arithmetic as a plan's frame, so each stream's output equals
 // the plan's.  The streams are spread over the worker CUDA streams, largest
 // first onto the least loaded worker, forked from and joined into `s`.
@@ -324,10 +322,13 @@ cudaError_t launch_staged_step(bmfr_batch* b, const bmfr::BatchStepDesc& d, cuda
             e = bmfr::launch_fitter(g, f, J.job.nc, J.tmp, half_tmp, b->p.fp32_qr, fb.weights, fb.mins_maxs,
                                     fb.noise, b->d_status, ws);
         if (e == cudaSuccess)
-            e = bmfr::launch_wsacc_taa(g, f, J.job.second_alpha, J.taa_alpha, fb.weights, fb.mins_maxs, fb.cur_n,
-                                       fb.cur_p, fb.prev_pix, fb.accept, fb.albedo, fb.cur_spp, fb.acc_prev,
-                                       fb.acc_cur, nullptr, nullptr, J.result_hist, J.result_prev, J.result_out,
-                                       half_hist, ws);
+            e = bmfr::launch_weighted_sum_accumulate(g, f, J.job.second_alpha, fb.weights, fb.mins_maxs, fb.cur_n,
+                                                     fb.cur_p, nullptr, fb.prev_pix, fb.accept, fb.albedo,
+                                                     fb.tone_mapped, fb.cur_spp, fb.acc_prev, fb.acc_cur, half_hist,
+                                                     ws);
+        if (e == cudaSuccess)
+            e = bmfr::launch_taa(g, f, J.taa_alpha, fb.prev_pix, fb.tone_mapped, J.result_hist, J.result_prev,
+                                 J.result_out, half_hist, ws);
     }
     for (int w = 0; w < kStepWorkers && e == cudaSuccess; ++w) {
         if (!used[w]) continue;

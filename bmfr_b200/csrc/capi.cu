@@ -63,7 +63,7 @@ struct bmfr_plan {
     const float* last_result = nullptr;         // float32 output of the last frame
     bool profiling = false;
     bool profiled_frame = false;
-    bool keep_intermediates = false;            // also write the filtered and tone-mapped frames
+    bool keep_intermediates = false;            // also write the filtered frame
     cudaEvent_t events[6] = {};                 // stage boundaries of the last frame
     // Ordering of uploads, frames and downloads that run on different
     // streams: input set k uploaded, frame f done (index f % 3), result of
@@ -533,19 +533,21 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
                                     plan->dev_status, s);
         mark(2);
     }
-    float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
-    // Both pipelines end with weighted_sum, accumulate_filtered_data and taa
-    // in one kernel: the filtered and tone-mapped frames stay on chip unless
-    // kept for inspection (bmfr_plan_keep_intermediates).
-    const bool keep = plan->keep_intermediates;
+    // weighted_sum and accumulate_filtered_data in one pass per pixel; the
+    // filtered colour is written only when kept for inspection
+    // (bmfr_plan_keep_intermediates).
     if (e == cudaSuccess)
-        e = bmfr::launch_wsacc_taa(g, f, plan->p.second_blend_alpha, plan->p.taa_blend_alpha, plan->weights,
-                                   plan->mins_maxs, cur_n, cur_p, plan->prev_pix, plan->accept, albedo,
-                                   plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur],
-                                   keep ? plan->filtered : nullptr, keep ? plan->tone_mapped : nullptr,
-                                   plan->result[cur], plan->result[prv], f32_out, half_hist, s);
+        e = bmfr::launch_weighted_sum_accumulate(g, f, plan->p.second_blend_alpha, plan->weights, plan->mins_maxs,
+                                                 cur_n, cur_p, plan->keep_intermediates ? plan->filtered : nullptr,
+                                                 plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
+                                                 plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur], half_hist,
+                                                 s);
     mark(3);
     mark(4);
+    float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
+    if (e == cudaSuccess)
+        e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped, plan->result[cur],
+                             plan->result[prv], f32_out, half_hist, s);
     mark(5);
     if (e == cudaSuccess) e = cudaEventRecord(plan->ev_frame_done[f % 3], s);
     if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
@@ -674,7 +676,7 @@ int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* b) {
     b->mins_maxs = plan->mins_maxs;
     b->filtered = plan->keep_intermediates ? plan->filtered : nullptr;
     b->prev_frame_pixel = reinterpret_cast<const float*>(plan->prev_pix);
-    b->tone_mapped = plan->keep_intermediates ? plan->tone_mapped : nullptr;
+    b->tone_mapped = plan->tone_mapped;
     b->accept = plan->accept;
     b->spp = plan->spp[last];
     b->accumulated_noisy = plan->noisy_acc[last];

@@ -5,8 +5,9 @@
 // tmp_data never reaches memory.  With `pixels` the same CTA then runs
 // weighted_sum + accumulate_filtered_data for the block's in-image pixels
 // (bmfr.cl:703-857) from the weights in shared memory; without it (the plan
-// pipeline) those stages run with TAA in the tile pass (k_wsacc_taa), where
-// they are not held to the fitter's three CTAs per SM.
+// pipeline) those stages run as the plan's per-pixel kernel
+// (k_weighted_sum_accumulate), which is not held to the fitter's three CTAs
+// per SM.
 //
 // The margin grid is tiled exactly by the fitter's blocks, and a pixel's
 // weights come from the block whose margin grid holds it unmirrored

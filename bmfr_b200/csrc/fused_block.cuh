@@ -29,9 +29,8 @@ __device__ __forceinline__ void tile_set1(Tile<false>& t, int k, int q, float v)
 // reference's tmp_data stores them (bmfr.cl:471-475); HistT: element type of
 // the colour histories.  PIXELS: phase 3 (weighted sum and filtered
 // accumulation of the block's in-image pixels) runs here; without it the
-// block ends at the fit and a pass over image tiles runs them with TAA
-// (wsacc_taa_tile).  Block b of job j; ends with every thread past the
-// fit's final barrier.
+// block ends at the fit and a per-pixel kernel runs them.  Block b of job j;
+// ends with every thread past the fit's final barrier.
 template <int METHOD, bool HALF_TMP, typename HistT, bool PIXELS = true>
 __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, FitterSmem& sm, float* w_s,
                                                  float* mm_s) {

@@ -76,16 +76,6 @@ cudaError_t launch_weighted_sum_accumulate(const Geometry& g, int frame, float s
                                            const uint8_t* cur_spp, const void* acc_prev, void* acc_cur,
                                            bool half_history, cudaStream_t s);
 
-// weighted_sum + accumulate_filtered_data + taa in one kernel (tiles with a
-// one-pixel ring recomputed); filtered and tone_mapped may be null (not
-// written), result_f32 may be null.
-cudaError_t launch_wsacc_taa(const Geometry& g, int frame, float second_alpha, float taa_alpha,
-                             const float* weights, const float* mins_maxs, const float* cur_n, const float* cur_p,
-                             const float2* prev_pix, const uint8_t* accept, const float* albedo,
-                             const uint8_t* cur_spp, const void* acc_prev, void* acc_cur, float* filtered,
-                             float* tone_mapped, void* result, const void* result_prev, float* result_f32,
-                             bool half_history, cudaStream_t s);
-
 cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const float2* prev_pix,
                        const float* new_frame, void* result, const void* prev_frame, float* result_f32,
                        bool half_history, cudaStream_t s);

@@ -412,71 +412,6 @@ __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float ta
     }
 }
 
-// weighted_sum + accumulate_filtered_data + taa of the image tile of
-// kWtTileW x kWtTileH pixels at (x0, y0), by one CTA (any thread count).
-// TAA reads the tone-mapped 3x3 neighbourhood (bmfr.cl:884-902), so the CTA
-// computes the first two stages for its tile plus a one-pixel ring around
-// it (the ring's pixels belong to the neighbouring tiles, which compute them
-// too: the same inputs give the same bits) and keeps their YCoCg and colour
-// in shared memory (s_ycc, s_rgb: kWtRingPixels each); the tone-mapped
-// frame then never goes to memory.  Phase 1: ring and tile, one pixel per
-// thread and iteration, the tile's accumulated colour (and, when not null,
-// its filtered and tone-mapped colours) written out.  Phase 2: TAA of the
-// tile's pixels from shared memory, in the reference's neighbour order
-// (taa_core).  Ends past a barrier, so the caller may reuse the arrays.
-constexpr int kWtTileW = 32, kWtTileH = 8;
-constexpr int kWtRingPixels = (kWtTileW + 2) * (kWtTileH + 2);
-
-template <typename HistT>
-__device__ __forceinline__ void wsacc_taa_tile(
-    const Geometry& g, int frame, float second_alpha, float taa_alpha, const float* __restrict__ weights,
-    const float* __restrict__ mins_maxs, const float* __restrict__ cur_n, const float* __restrict__ cur_p,
-    const float2* __restrict__ prev_pix, const uint8_t* __restrict__ accept, const float* __restrict__ albedo,
-    const uint8_t* __restrict__ cur_spp, const HistT* __restrict__ acc_prev, HistT* __restrict__ acc_cur,
-    float* __restrict__ filtered, float* __restrict__ tone_mapped, HistT* __restrict__ result,
-    const HistT* __restrict__ result_prev, float* __restrict__ result_f32, int x0, int y0, float4* s_ycc,
-    float4* s_rgb) {
-    constexpr int RW = kWtTileW + 2;
-    for (int i = threadIdx.x; i < kWtRingPixels; i += blockDim.x) {
-        const int rx = i % RW, ry = i / RW;
-        const int x = x0 - 1 + rx, y = y0 - 1 + ry;
-        if (x < 0 || y < 0 || x >= g.W || y >= g.H) continue;   // never read: taa skips such neighbours
-        float3 f, tm;
-        const float3 a3 = wsacc_core<HistT>(g, frame, second_alpha, x, y, weights, mins_maxs, cur_n, cur_p,
-                                            prev_pix, accept, albedo, cur_spp, acc_prev, &f, &tm);
-        if (rx >= 1 && rx <= kWtTileW && ry >= 1 && ry <= kWtTileH) {
-            const int lp = y * g.W + x;
-            hist_store(acc_cur, lp, a3);
-            if (filtered) store3(filtered, lp, f);
-            if (tone_mapped) store3(tone_mapped, lp, tm);
-        }
-        float c[3];
-        rgb_to_ycocg(tm, c);
-        s_ycc[i] = make_float4(c[0], c[1], c[2], 0.0f);
-        s_rgb[i] = make_float4(tm.x, tm.y, tm.z, 0.0f);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kWtTileW * kWtTileH; i += blockDim.x) {
-        const int tx = i % kWtTileW, ty = i / kWtTileW;
-        const int x = x0 + tx, y = y0 + ty;
-        if (x >= g.W || y >= g.H) continue;
-        const int lp = y * g.W + x;
-        const int c0 = (ty + 1) * RW + tx + 1;
-        const float4 m = s_rgb[c0];
-        auto nb = [&](int dx, int dy, float (&ycc)[3]) {
-            const float4 v = s_ycc[c0 + dy * RW + dx];
-            ycc[0] = v.x;
-            ycc[1] = v.y;
-            ycc[2] = v.z;
-        };
-        const float3 out = taa_core<HistT>(g, frame, taa_alpha, x, y, prev_pix[lp], make_float3(m.x, m.y, m.z), nb,
-                                           result_prev);
-        hist_store(result, lp, out);
-        if (result_f32) store3(result_f32, lp, out);
-    }
-    __syncthreads();
-}
-
 // taa of one pixel, neighbours read from global memory.
 template <typename HistT>
 __device__ __forceinline__ float3 taa_px(const Geometry& g, int frame, float taa_alpha, int px, int py,

@@ -131,23 +131,6 @@ __global__ void __launch_bounds__(128) k_taa(Geometry g, int frame, float taa_al
                                prev_pix, new_frame, prev_frame, result, result_f32);
 }
 
-// Fused weighted_sum + accumulate_filtered_data + taa: one CTA per tile of
-// kWtTileW x kWtTileH image pixels (wsacc_taa_tile, pixel_ops.cuh).
-template <typename HistT>
-__global__ void __launch_bounds__(256, 4) k_wsacc_taa(
-    Geometry g, int frame, float second_alpha, float taa_alpha, const float* __restrict__ weights,
-    const float* __restrict__ mins_maxs, const float* __restrict__ cur_n, const float* __restrict__ cur_p,
-    const float2* __restrict__ prev_pix, const uint8_t* __restrict__ accept, const float* __restrict__ albedo,
-    const uint8_t* __restrict__ cur_spp, const HistT* __restrict__ acc_prev, HistT* __restrict__ acc_cur,
-    float* __restrict__ filtered, float* __restrict__ tone_mapped, HistT* __restrict__ result,
-    const HistT* __restrict__ result_prev, float* __restrict__ result_f32) {
-    await_previous_kernel();
-    __shared__ float4 s_ycc[kWtRingPixels], s_rgb[kWtRingPixels];
-    wsacc_taa_tile<HistT>(g, frame, second_alpha, taa_alpha, weights, mins_maxs, cur_n, cur_p, prev_pix, accept,
-                          albedo, cur_spp, acc_prev, acc_cur, filtered, tone_mapped, result, result_prev, result_f32,
-                          blockIdx.x * kWtTileW, blockIdx.y * kWtTileH, s_ycc, s_rgb);
-}
-
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -210,24 +193,6 @@ cudaError_t launch_weighted_sum_accumulate(const Geometry& g, int frame, float s
     return launch_chained(k_weighted_sum_accumulate<float>, image_grid(g), dim3(32, 8), 0, s, g, frame, second_alpha,
                           weights, mins_maxs, cur_n, cur_p, filtered, prev_pix, accept, albedo, tone_mapped, cur_spp,
                           (const float*)acc_prev, (float*)acc_cur);
-}
-
-cudaError_t launch_wsacc_taa(const Geometry& g, int frame, float second_alpha, float taa_alpha,
-                             const float* weights, const float* mins_maxs, const float* cur_n, const float* cur_p,
-                             const float2* prev_pix, const uint8_t* accept, const float* albedo,
-                             const uint8_t* cur_spp, const void* acc_prev, void* acc_cur, float* filtered,
-                             float* tone_mapped, void* result, const void* result_prev, float* result_f32,
-                             bool half_history, cudaStream_t s) {
-    const dim3 grid((g.W + kWtTileW - 1) / kWtTileW, (g.H + kWtTileH - 1) / kWtTileH), block(256);
-    if (half_history)
-        return launch_chained(k_wsacc_taa<__half>, grid, block, 0, s, g, frame, second_alpha, taa_alpha,
-                              weights, mins_maxs, cur_n, cur_p, prev_pix, accept, albedo, cur_spp,
-                              (const __half*)acc_prev, (__half*)acc_cur, filtered, tone_mapped, (__half*)result,
-                              (const __half*)result_prev, result_f32);
-    return launch_chained(k_wsacc_taa<float>, grid, block, 0, s, g, frame, second_alpha, taa_alpha, weights,
-                          mins_maxs, cur_n, cur_p, prev_pix, accept, albedo, cur_spp, (const float*)acc_prev,
-                          (float*)acc_cur, filtered, tone_mapped, (float*)result, (const float*)result_prev,
-                          result_f32);
 }
 
 cudaError_t launch_taa(const Geometry& g, int frame, float taa_alpha, const float2* prev_pix,

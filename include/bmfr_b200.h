@@ -60,8 +60,8 @@ extern "C" {
 #define BMFR_PIPELINE_STAGED 0  /* the five stage kernels, reference order   */
 #define BMFR_PIPELINE_FUSED 1   /* accumulate+fit in one kernel per 32x32
                                    block (tmp_data stays on chip), then
-                                   weighted sum+filtered accumulation+TAA
-                                   in one kernel over image tiles            */
+                                   weighted sum+filtered accumulation, then
+                                   TAA                                       */
 
 /* Runtime form of the reference's compile-time options.  Defaults
  * (bmfr_params_default) are the reference's values.  */
@@ -280,8 +280,8 @@ int bmfr_plan_reset(bmfr_plan* plan);   /* frame counter back to 0 */
 
 /* Intermediate buffers of the last frame, for inspection and tests.  Which
  * pointers exist depends on the pipeline: the fused pipeline keeps no
- * tmp_data (NULL); both pipelines run weighted_sum, accumulate_filtered_data
- * and taa as one kernel, so the filtered and tone-mapped frames are written
+ * tmp_data (NULL); both pipelines run weighted_sum and
+ * accumulate_filtered_data as one kernel, whose filtered frame is written
  * (non-NULL here) only while bmfr_plan_keep_intermediates is on. */
 typedef struct bmfr_plan_buffers {
     const void* tmp_data;
@@ -292,10 +292,10 @@ typedef struct bmfr_plan_buffers {
     const float* result;
 } bmfr_plan_buffers;
 int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* buffers);
-/* Enable (1) or disable (0, the default) writing the filtered and
- * tone-mapped frames of every frame, which the reference keeps in global
- * buffers (bmfr.cpp:331-340) and the plan otherwise keeps on chip.  Outputs
- * are the same either way. */
+/* Enable (1) or disable (0, the default) writing the filtered frame of
+ * every frame, which the reference keeps in a global buffer (bmfr.cpp:331)
+ * and the plan otherwise keeps on chip between weighted_sum and
+ * accumulate_filtered_data.  Outputs are the same either way. */
 int bmfr_plan_keep_intermediates(bmfr_plan* plan, int enable);
 
 /* Per-stage timing of the plan pipeline, in place of the reference's
@@ -303,11 +303,11 @@ int bmfr_plan_keep_intermediates(bmfr_plan* plan, int enable);
  * enabled, every denoise call records CUDA events between its stages.
  * bmfr_plan_stage_times waits for the last frame and returns milliseconds of
  * the staged pipeline's [accumulate_noisy_data (with the frame's fitter
- * noise table), fitter, weighted_sum + accumulate_filtered_data + taa (one
- * kernel in the plan pipeline), 0, 0].  The fused pipeline reports [noise table,
+ * noise table), fitter, weighted_sum + accumulate_filtered_data (one kernel
+ * in the plan pipeline), 0, taa].  The fused pipeline reports [noise table,
  * block kernel (accumulate and fitter), weighted_sum +
- * accumulate_filtered_data + taa, 0, 0].  The five drop-in stage entry
- * points time separately with events around each call. */
+ * accumulate_filtered_data, 0, taa].  The five drop-in stage entry points
+ * time separately with events around each call. */
 #define BMFR_STAGE_COUNT 5
 int bmfr_plan_enable_profiling(bmfr_plan* plan, int enable);
 int bmfr_plan_stage_times(const bmfr_plan* plan, float ms[BMFR_STAGE_COUNT]);

@@ -53,10 +53,9 @@ typedef struct bmfr_batch_tuning {
                                into L2.  The staged step launches a plan's kernels, whose
                                shapes are fixed: it has nothing to tune. */
     int pixel_pass;         /* fused step: 0 runs weighted sum + filtered accumulation in the
-                               block kernel after each block's fit, then TAA over 30-column
-                               strips; 1 ends the block kernel at the fit and runs weighted
-                               sum + filtered accumulation + TAA as one pass over 32x8 image
-                               tiles (the taa_tile fields are then unused) */
+                               block kernel after each block's fit; 1 ends the block kernel at
+                               the fit and runs them as a launch over every stream's 32x8
+                               pixel tiles.  TAA follows either way. */
 } bmfr_batch_tuning;
 
 /* memory_budget_bytes: device bytes the batch's streams may hold (0: no limit).

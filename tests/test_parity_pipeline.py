@@ -80,10 +80,9 @@ def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
 
 @pytest.mark.parametrize("half_history", [0, 1])
 def test_kept_intermediates_change_no_output(cuda, half_history):
-    """The staged pipeline runs weighted sum, filtered accumulation and TAA as
-    one kernel; writing its filtered and tone-mapped frames out for
-    inspection must not change any output bit, and those frames must equal
-    the drop-in entry points' on the same frame."""
+    """The plan runs weighted sum and filtered accumulation as one kernel;
+    writing its filtered frame out for inspection must not change any output
+    bit, and that frame must equal the drop-in weighted_sum's."""
     import torch
     W, H = 200, 120
     sc = B.Scene(24, W, H, 12)
@@ -91,7 +90,7 @@ def test_kept_intermediates_change_no_output(cuda, half_history):
               position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared)
     plain, kept = B.Plan(W, H, **kw), B.Plan(W, H, **kw)
     kept.keep_intermediates(True)
-    assert plain.buffers().tone_mapped is None and plain.buffers().filtered is None
+    assert plain.buffers().filtered is None and kept.buffers().filtered is not None
     for f in range(4):
         d = sc.render(f)
         for pl in (plain, kept):
@@ -102,9 +101,8 @@ def test_kept_intermediates_change_no_output(cuda, half_history):
         a, b = plain.buffers(), kept.buffers()
         np.testing.assert_array_equal(device_array(a.accumulated_filtered, (H, W, 3), hist),
                                       device_array(b.accumulated_filtered, (H, W, 3), hist))
-        # The kept frames are the drop-in weighted_sum's and
-        # accumulate_filtered_data's outputs (float histories only: the
-        # drop-in entry points take float buffers).
+        # The kept frame is the drop-in weighted_sum's output (float
+        # histories only: the drop-in entry points take float buffers).
         if not half_history and f > 0:
             n = W * H * 3
             t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).reshape(-1).to(cuda)
