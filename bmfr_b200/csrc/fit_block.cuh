@@ -49,6 +49,7 @@ struct FitterSmem {
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
     float part2[13 * 8];   // second-stage sums, 8 per batched value
+    float part1[64];       // first-stage sums of block_sum1_all
     float rowc[13];        // the precision form: row `col` of every column
     float inv1[10];        // CholeskyQR2: reciprocals of R1's and R2's diagonals,
     float inv2[10];        //   and the diagonal of the Gram matrix being factored
@@ -151,6 +152,38 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
         }
     }
     __syncthreads();
+}
+
+// parallel_reduction_sum (bmfr.cl:25-43) of one value per thread, finished by
+// every warp: stage 1 inside each warp on shuffles (ids i, i+64, i+128,
+// i+192), one barrier, then each warp reads the 64 first-stage sums and runs
+// stages 2 and 3 itself in the reference's order, so the sum reaches every
+// thread without a second barrier or a broadcast through shared memory.
+// part1 is rewritten only by the next call, and a batched block_reduce (two
+// barriers) separates consecutive calls in the column loop, so no warp can
+// overwrite sums another warp is still reading.
+__device__ __forceinline__ float block_sum1_all(float v, FitterSmem& sm) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float b = __shfl_down_sync(kFull, v, 8);
+    const float c = __shfl_down_sync(kFull, v, 16);
+    const float d = __shfl_down_sync(kFull, v, 24);
+    const float s1 = v + ((b + c) + d);   // bmfr.cl:33
+    if (lane < 8) sm.part1[8 * warp + lane] = s1;
+    __syncthreads();
+    // Stage 2 (bmfr.cl:35-37): lane j < 8 forms sum_vec[j].
+    float s2 = 0.0f;
+    if (lane < 8) {
+        const float* p = sm.part1 + lane;
+        float acc = p[8];
+#pragma unroll
+        for (int m = 2; m < 8; ++m) acc = acc + p[8 * m];
+        s2 = p[0] + acc;
+    }
+    // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right.
+    float r = __shfl_sync(kFull, s2, 0);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) r = r + __shfl_sync(kFull, s2, k);
+    return r;
 }
 
 // The block as held by one thread: four rows of the 13 columns.
@@ -305,9 +338,8 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
         s = s + c23.y * c23.y;
         nv[0] = s;
     }
-    if (id == col) sm.ucl = c01.x;
-    block_reduce<1, 0, 0>(nv, 1, 1, sm);
-    const float norm2 = sm.out[0];
+    if (id == col) sm.ucl = c01.x;   // read after block_sum1_all's barrier
+    const float norm2 = block_sum1_all(nv[0], sm);
     const float ucl = sm.ucl;
     // Work-item col's step (bmfr.cl:580-588), evaluated by every thread.
     const float vl = sqrtf(norm2 + ucl * ucl);

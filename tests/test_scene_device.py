@@ -11,7 +11,11 @@ construction, and the tolerances below follow from how they differ:
   (camera height h = 3, d_y = -h / t), so with float directions (error
   ~1e-7) the position of a pixel that hits the same object agrees to
   |dp| <= 1e-4 + 2e-7 t^2, t <= |p| + 10.5 (the camera's distance from the
-  origin); normals agree to |dn| <= 1e-4;
+  origin), on 99.9 % of the pixels; a ray that grazes a sphere has a small
+  discriminant b^2 - c, whose float rounding (b^2 ~ 100) sqrt magnifies, so
+  the few such pixels are held to |dp| <= 5e-3; a sphere's normal is
+  (p - c) / r, so where the position bound holds the normals agree to that
+  bound divided by the smallest radius (0.3), and the plane's are exact;
 * a grazing ray at an object's silhouette may hit another object (or
   nothing) in one of them: such pixels are counted (albedo differs, or one
   side misses) and must stay below 0.2 % of the image;
@@ -53,9 +57,12 @@ def test_device_render_matches_host_render(cuda, W, H, frames):
         dp = np.linalg.norm(got["positions"] - host["positions"], axis=-1)[m]
         t = np.linalg.norm(host["positions"], axis=-1)[m] + 10.5
         bound = 1e-4 + 2e-7 * t * t
-        assert (dp <= bound).all(), f"frame {f}: positions {dp.max():.2e} (worst ratio {(dp / bound).max():.2f})"
-        dn = np.abs(got["normals"] - host["normals"])[m]
-        assert dn.max() <= 1e-4, f"frame {f}: normals {dn.max():.2e}"
+        ok = dp <= bound
+        assert ok.mean() >= 0.999, f"frame {f}: {(~ok).sum()} positions beyond the ray-length bound"
+        assert dp.max() <= 5e-3, f"frame {f}: positions {dp.max():.2e}"
+        dn = np.linalg.norm(got["normals"] - host["normals"], axis=-1)[m]
+        nbound = bound / 0.3 + 1e-5
+        assert (dn[ok] <= nbound[ok]).all(), f"frame {f}: normals {(dn[ok] / nbound[ok]).max():.2f} of the bound"
         # Misses are all zero on both sides.
         miss = same & ~hit_h
         for k in ("albedo", "normals", "positions", "noisy", "clean"):
