@@ -48,7 +48,6 @@ struct FitterSmem {
     int status;            // nonzero: a bounded wait ran out
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
-    float part2[13 * 8];   // second-stage sums, 8 per batched value
     float part1[64];       // first-stage sums of block_sum1_all
     float rowc[13];        // the precision form: row `col` of every column
     float inv1[10];        // CholeskyQR2: reciprocals of R1's and R2's diagonals,
@@ -139,17 +138,16 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
         }
     }
     // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right,
-    // by lane 0 of the group from shared memory.
+    // by lane 0 of the group from its lanes' values on shuffles.
     if (warp < n) {   // warp-uniform: warps without a value skip
-        if (vi < n) sm.part2[vi * 8 + j] = s2;
-        __syncwarp();
-        if (vi < n && j == 0) {
-            const float* p = sm.part2 + vi * 8;
-            float r = p[0];
+        const int base = lane & ~7;
+        float r = __shfl_sync(kFull, s2, base);
 #pragma unroll
-            for (int m = 1; m < 8; ++m) r = op == 0 ? r + p[m] : (op == 1 ? fmin_cl(r, p[m]) : fmax_cl(r, p[m]));
-            sm.out[vi] = r;
+        for (int m = 1; m < 8; ++m) {
+            const float x = __shfl_sync(kFull, s2, base + m);
+            r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
         }
+        if (vi < n && j == 0) sm.out[vi] = r;
     }
     __syncthreads();
 }
@@ -398,9 +396,13 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
             float2 n01, n23;
             if (fast) {
+                // The numerator and the first quotient estimate feed only
+                // multiplies and fused multiply-adds, never an add, so the
+                // packed multiply cannot be contracted here and rounds each
+                // lane as the reference's multiplication does.
                 const float2 d2 = dup2(dot);
-                const float2 num01 = rmul2(u2_01, d2), num23 = rmul2(u2_23, d2);
-                const float2 nq01 = rmul2(num01, ny), nq23 = rmul2(num23, ny);
+                const float2 num01 = mul2(u2_01, d2), num23 = mul2(u2_23, d2);
+                const float2 nq01 = mul2(num01, ny), nq23 = mul2(num23, ny);
                 const float2 r01 = fma2(nq01, b2, num01), r23 = fma2(nq23, b2, num23);
                 n01 = add2(a01, fma2(r01, ny, nq01));
                 n23 = add2(a23, fma2(r23, ny, nq23));

@@ -26,7 +26,12 @@ construction, and the tolerances below follow from how they differ:
   the channels, and a firefly decision (a uniform below 0.001, a factor of
   100 when it differs) may differ only where a uniform lies within 2^-24 of
   the threshold: at most 1e-5 of the channels are off by more than 10 %;
-* the albedo is copied from the same table: exact where the object agrees.
+* the albedo is copied from the same table: exact where the object agrees;
+* the noise-free image is clamp(pow(albedo * (max(0, n.l) + 0.1), 0.4545)),
+  whose slope in the normal is at most 0.4545 x^-0.545 * albedo <= 8 for
+  albedo in [0.05, 0.95] and shading >= 0.1, so it agrees to 1e-4 plus 8
+  times the normal bound where the position bound holds, and to 0.05 on the
+  grazing pixels.
 """
 import numpy as np
 import pytest
@@ -70,5 +75,7 @@ def test_device_render_matches_host_render(cuda, W, H, frames):
         rel = np.abs(got["noisy"] - host["noisy"])[m] / np.maximum(np.abs(host["noisy"][m]), 1e-6)
         assert np.quantile(rel, 0.9999) <= 1e-3, f"frame {f}: noisy {np.quantile(rel, 0.9999):.2e}"
         assert (rel > 0.1).mean() <= 1e-5, f"frame {f}: {(rel > 0.1).sum()} channels off by more than 10 %"
-        dc = np.abs(got["clean"] - host["clean"])[m]
-        assert dc.max() <= 1e-4, f"frame {f}: clean {dc.max():.2e}"
+        dc = np.abs(got["clean"] - host["clean"])[m].max(axis=-1)
+        cbound = 1e-4 + 8.0 * nbound
+        assert (dc[ok] <= cbound[ok]).all(), f"frame {f}: clean {(dc[ok] / cbound[ok]).max():.2f} of the bound"
+        assert dc.max() <= 0.05, f"frame {f}: clean {dc.max():.2e}"
