@@ -238,6 +238,7 @@ cudaError_t launch_batch_wsacc(const BatchStepDesc* desc, bool half_history, int
 
 cudaError_t launch_batch_taa(const BatchStepDesc* desc, bool half_history, const BatchTuning& t, int sms,
                              cudaStream_t s) {
+    if (t.tile_h == 8) return launch_taa_t<2>(desc, half_history, sms, s);
     if (t.tile_h == 16) return launch_taa_t<4>(desc, half_history, sms, s);
     if (t.tile_h == 64) return launch_taa_t<16>(desc, half_history, sms, s);
     return launch_taa_t<8>(desc, half_history, sms, s);

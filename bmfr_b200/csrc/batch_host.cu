@@ -722,8 +722,9 @@ int bmfr_batch_get_tuning(const bmfr_batch* b, bmfr_batch_tuning* t) {
 int bmfr_batch_set_tuning(bmfr_batch* b, const bmfr_batch_tuning* t) {
     if (int st = check_batch(b)) return st;
     if (!t) return fail(BMFR_E_INVALID, "tuning is NULL");
-    const bool shape_ok = t->taa_tile_w == 30 && (t->taa_tile_h == 16 || t->taa_tile_h == 32 || t->taa_tile_h == 64);
-    if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 30x16, 30x32 or 30x64");
+    const bool shape_ok = t->taa_tile_w == 30 && (t->taa_tile_h == 8 || t->taa_tile_h == 16 || t->taa_tile_h == 32 ||
+                                                  t->taa_tile_h == 64);
+    if (!shape_ok) return fail(BMFR_E_INVALID, "TAA tile shape must be 30x8, 30x16, 30x32 or 30x64");
     if (t->block_ctas_per_sm < 0 || t->staging_depth < 0 || t->staging_depth > 4)
         return fail(BMFR_E_INVALID, "bad block CTAs per SM or staging depth");
     if (t->pixel_pass != 0 && t->pixel_pass != 1) return fail(BMFR_E_INVALID, "pixel_pass must be 0 or 1");
@@ -783,8 +784,8 @@ int bmfr_batch_autotune(bmfr_batch* b, int n, const int* slots, const bmfr_frame
             }
         }
     }
-    const int shapes[2][2] = {{30, 16}, {30, 64}};
-    for (int i = 0; i < 2 && status == BMFR_OK; ++i) {
+    const int shapes[3][2] = {{30, 8}, {30, 16}, {30, 64}};
+    for (int i = 0; i < 3 && status == BMFR_OK; ++i) {
         bmfr_batch_tuning t = best;
         t.taa_tile_w = shapes[i][0];
         t.taa_tile_h = shapes[i][1];

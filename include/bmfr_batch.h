@@ -46,7 +46,7 @@ typedef struct bmfr_batch bmfr_batch;
 typedef struct bmfr_batch_tuning {
     int block_ctas_per_sm;  /* fused step: persistent CTAs of the block kernel per SM
                                (0: as many as fit) */
-    int taa_tile_w;         /* fused step's TAA CTA tile: 30 columns x 16, 32 or 64 rows */
+    int taa_tile_w;         /* fused step's TAA CTA tile: 30 columns x 8, 16, 32 or 64 rows */
     int taa_tile_h;
     int staging_depth;      /* fused step: 0 takes blocks from an atomic queue; k > 0 a static
                                order with the inputs of each CTA's next k blocks prefetched

@@ -181,7 +181,7 @@ def test_batch_autotune_and_budget(cuda, pipeline):
     mats = np.concatenate([s.sc.prev_camera(0) for s in streams])
     offs = np.concatenate([s.sc.pixel_offset(0) for s in streams])
     t, ms = batch.autotune(slots, mats, offs, io=io, steps=1)
-    assert ms > 0 and (t.taa_tile_w, t.taa_tile_h) in [(30, 16), (30, 32), (30, 64)]
+    assert ms > 0 and (t.taa_tile_w, t.taa_tile_h) in [(30, 8), (30, 16), (30, 32), (30, 64)]
     if pipeline == B.PIPELINE_FUSED:
         assert 0 <= t.staging_depth <= 2 and t.block_ctas_per_sm >= 1
     else:   # the staged step launches the plan's kernels: nothing to tune

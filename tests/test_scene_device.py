@@ -22,10 +22,13 @@ construction, and the tolerances below follow from how they differ:
 * the noise draws come from the same 64-bit counter hash, as a 24-bit
   uniform on the device and a 53-bit one on the host; Box-Muller's log and
   cos then agree to ~1e-6 except where the uniform is tiny (the far tail of
-  the lognormal), so the 1-spp colour is within 1e-3 relative for 99.99 % of
-  the channels, and a firefly decision (a uniform below 0.001, a factor of
-  100 when it differs) may differ only where a uniform lies within 2^-24 of
-  the threshold: at most 1e-5 of the channels are off by more than 10 %;
+  the lognormal); the colour also carries the shading max(0, n.l) + 0.1 >=
+  0.1, whose relative error is at most 10 times the normal's, so where the
+  position bound holds the 1-spp colour is within 1e-4 + 10 times the normal
+  bound, relative, on 99.99 % of the channels, and a firefly decision (a
+  uniform below 0.001, a factor of 100 when it differs) may differ only where
+  a uniform lies within 2^-24 of the threshold: at most 1e-5 of the channels
+  are off by more than 10 %;
 * the albedo is copied from the same table: exact where the object agrees;
 * the noise-free image is clamp(pow(albedo * (max(0, n.l) + 0.1), 0.4545)),
   whose slope in the normal is at most 0.4545 x^-0.545 * albedo <= 8 for
@@ -73,7 +76,9 @@ def test_device_render_matches_host_render(cuda, W, H, frames):
         for k in ("albedo", "normals", "positions", "noisy", "clean"):
             assert (got[k][miss] == 0).all() and (host[k][miss] == 0).all(), k
         rel = np.abs(got["noisy"] - host["noisy"])[m] / np.maximum(np.abs(host["noisy"][m]), 1e-6)
-        assert np.quantile(rel, 0.9999) <= 1e-3, f"frame {f}: noisy {np.quantile(rel, 0.9999):.2e}"
+        rbound = (1e-4 + 10.0 * nbound)[:, None]
+        within = (rel <= rbound)[ok]
+        assert within.mean() >= 0.9999, f"frame {f}: {(~within).sum()} colour channels beyond the bound"
         assert (rel > 0.1).mean() <= 1e-5, f"frame {f}: {(rel > 0.1).sum()} channels off by more than 10 %"
         dc = np.abs(got["clean"] - host["clean"])[m].max(axis=-1)
         cbound = 1e-4 + 8.0 * nbound
