@@ -74,7 +74,7 @@ __device__ __forceinline__ void fused_block_body(const BlockJob& j, int b, Fitte
         const float3 wp = load3(cur_p, lp);
         const float3 nrm = load3(cur_n, lp);
         const float3 cur = load3(noisy_in, lp);
-        const AccumResult r = accumulate_core<HistT>(g, a, px, py, wp, nrm, cur, prev_n, prev_p, noisy_acc_prev,
+        const AccumResult r = accumulate_core<HistT, true>(g, a, px, py, wp, nrm, cur, prev_n, prev_p, noisy_acc_prev,
                                                      prev_spp);
         if (in_image) {   // bmfr.cl:442, 478-484
             owned |= 1u << q;

@@ -3,6 +3,8 @@
 // expression keeps the reference's operation order.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace bmfr {
@@ -21,7 +23,13 @@ struct AccumResult {
 
 // Reprojection, 4-tap history gather and blend of one pixel
 // (bmfr.cl:319-445).  `cur` is the pixel's colour before blending.
-template <typename HistT>
+// PREFETCH: the previous positions and normals of all in-image taps are
+// loaded before any tap is tested, so their latencies overlap (more
+// registers); the tests and the blend keep the reference's order either
+// way.  Measured on the float-history pipeline at 1280x720: 159.1 -> 156.2 us
+// per frame, and 184.7 -> 170.2 us in the fused block kernel; with binary16
+// histories it lost (1080p 218.4 -> 220.4 us), so it is off there.
+template <typename HistT, bool PREFETCH = std::is_same<HistT, float>::value>
 __device__ __forceinline__ AccumResult accumulate_core(
     const Geometry& g, const AccumArgs& a, int px, int py, float3 wp, float3 nrm, float3 cur,
     const float* __restrict__ prev_n, const float* __restrict__ prev_p,
@@ -49,15 +57,25 @@ __device__ __forceinline__ AccumResult accumulate_core(
         const float ofx = 1.0f - fx, ofy = 1.0f - fy;
         const float wts[4] = {ofx * ofy, fx * ofy, ofx * fy, fx * fy};
         float total = 0.0f;
+        float3 tp[4], tn[4];
+        int ts[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int sx = ix + (i & 1), sy = iy + (i >> 1);
-            if (sx >= 0 && sy >= 0 && sx < g.W && sy < g.H) {
-                const int s = sy * g.W + sx;
-                const float3 pp = load3(prev_p, s);
+            ts[i] = (sx >= 0 && sy >= 0 && sx < g.W && sy < g.H) ? sy * g.W + sx : -1;
+            if (PREFETCH && ts[i] >= 0) {
+                tp[i] = load3(prev_p, ts[i]);
+                tn[i] = load3(prev_n, ts[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (ts[i] >= 0) {
+                const int s = ts[i];
+                const float3 pp = PREFETCH ? tp[i] : load3(prev_p, s);
                 const float dx = pp.x - wp.x, dy = pp.y - wp.y, dz = pp.z - wp.z;
                 if ((dx * dx + dy * dy) + dz * dz < a.pos_lim2) {
-                    const float3 pn = load3(prev_n, s);
+                    const float3 pn = PREFETCH ? tn[i] : load3(prev_n, s);
                     const float ex = pn.x - nrm.x, ey = pn.y - nrm.y, ez = pn.z - nrm.z;
                     if ((ex * ex + ey * ey) + ez * ez < a.nrm_lim2) {
                         r.accept |= (uint8_t)(1 << i);
