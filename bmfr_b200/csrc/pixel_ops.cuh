@@ -381,6 +381,15 @@ __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float ta
     const bool writer = lane >= 1 && lane <= 30 && col_in;
     float3 rgb[3];
     float cmn[3][3], cmx[3][3], hmn[3][3], hmx[3][3];   // [window row][channel]
+    // The strip's reprojected positions first: the history gather of each
+    // row depends on them, and they depend on nothing here (1920x1080
+    // frame 319.4 -> 315.2 us).
+    float2 ppre[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+        const int py = y0 + rr;
+        ppre[rr] = (writer && py < g.H) ? prev_pix[py * g.W + x] : make_float2(0.f, 0.f);
+    }
 #pragma unroll
     for (int r = 0; r < R + 2; ++r) {
         const int k = r % 3;
@@ -408,7 +417,7 @@ __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float ta
             const int py = y0 + r - 2;
             if (writer && py < g.H) {
                 const int lp = py * g.W + x;
-                const float2 pp = prev_pix[lp];
+                const float2 pp = ppre[r - 2];
                 const float3 mine = rgb[mid];
                 const int ix = floor_to_int(pp.x), iy = floor_to_int(pp.y);
                 float3 out = mine;
