@@ -1260,6 +1260,29 @@ def main():
     stage_gbs = {k: sb[k] / (v * 1e-3) / 1e9 for k, v in stages.items() if v > 0}
     dropin = dropin_stage_ms(B, torch, dev, stream, plan.params, devf, mats, off, min(args.steps, 30))
 
+    # ---- the other plan pipeline on the same frames, beside the bench's ----
+    other = B.PIPELINE_STAGED if pipeline == B.PIPELINE_FUSED else B.PIPELINE_FUSED
+    oplan = B.Plan(WIDTH, HEIGHT, pipeline=other, position_limit_squared=sc.position_limit_squared,
+                   normal_limit_squared=sc.normal_limit_squared)
+
+    def other_steps(loop):
+        for i in range(args.steps):
+            k = loop * args.steps + i
+            f = frame_order(k, nfr)
+            pf = frame_order(k - 1, nfr) if k > 0 else f
+            oplan.denoise_frame_io(devf["albedo"][f], devf["normals"][f], devf["positions"][f], devf["noisy"][f],
+                                   devf["normals"][pf], devf["positions"][pf], mats[pf], off, stream=stream)
+
+    other_steps(0)
+    stream.synchronize()
+    other_ms = max_over_ranks(statistics.median(timed_loops(other_steps, stream, dev, min_seconds=0.2)), device=dev)
+    oplan.close()
+    other_line = {"pipeline": "fused" if other == B.PIPELINE_FUSED else "staged",
+                  "value": world * args.steps / (other_ms / 1e3), "unit": "frames/s",
+                  "ms_per_step": other_ms / args.steps,
+                  "how": "fused: accumulate + fit in one kernel per 32x32 block (tmp_data stays on chip), then "
+                         "weighted sum + filtered accumulation, then TAA; staged: the four-kernel plan pipeline"}
+
     # ---- e2e: host buffers through the C ABI --------------------------------
     # Uploads, frames and downloads on three streams: the plan orders them,
     # so frame i+1's upload and frame i-1's download overlap frame i.
@@ -1317,7 +1340,7 @@ def main():
                        "width": WIDTH, "height": HEIGHT, "frames": nfr, "pipeline": args.pipeline,
                        "tmp_data": "binary16", "parallelism": f"replicas x{world}",
                        "l2": "no flush: per-frame working set ~180 MB (inputs + histories) exceeds the 126 MB L2"},
-            "stages_ms": stages, "stages_gbs": stage_gbs,
+            "stages_ms": stages, "stages_gbs": stage_gbs, "other_pipeline": other_line,
             "dropin_stages_ms": dropin,
             "dropin_stages_gbs": {k: sb[k] / (v * 1e-3) / 1e9 for k, v in dropin.items() if v > 0},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
