@@ -66,6 +66,7 @@ struct AccumArgs {
 // once to float without double arithmetic on the device.
 struct NoiseConst {
     float hi, lo;
+    float neg_zero;   // -0.0f, known only at run time: the addend of the fitter's products (rmul2)
 };
 
 // OpenCL's fmin/fmax (and max(x, y) for the operands the kernels give it):

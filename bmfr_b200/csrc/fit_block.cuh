@@ -14,13 +14,14 @@
 // so that the first stage of the reference's reduction tree (ids i, i+64,
 // i+128, i+192, bmfr.cl:32-33) sits inside one warp and runs on shuffles.
 //
-// Reductions.  block_reduce evaluates parallel_reduction_sum/min/max
-// (bmfr.cl:25-87) over exactly the same tree, so the sums round exactly as
-// the reference's do, and batches up to 12 independent reductions behind
-// one pair of barriers: the twelve min/max values of the scaling step, and
-// per column the up to twelve dot products, which are independent once the
-// Householder vector is known.  A column costs two batched reductions (norm,
-// dots) — four barriers — where the reference spends three per dot product.
+// Reductions.  block_reduce (min/max), block_sum_dots and block_sum1_all
+// evaluate parallel_reduction_sum/min/max (bmfr.cl:25-87) over exactly the
+// same tree, so the sums round exactly as the reference's do.  The batched
+// forms reduce up to 12 independent values behind one pair of barriers: the
+// twelve min/max values of the scaling step, and per column the up to twelve
+// dot products, which are independent once the Householder vector is known.
+// A column costs the norm (one barrier) and the dots (two) where the
+// reference spends three barriers per dot product.
 //
 // Columns run in a loop; after each column the register tile shifts down by
 // one column so that every index into it is a compile-time constant.
@@ -41,8 +42,13 @@
 
 namespace bmfr {
 
+// Row stride of FitterSmem::part: 64 first-stage sums per value plus three
+// floats of padding, so that the 8-lane groups storing values i and i + 6
+// (or i + 3) and the groups reading values v and v + 8 fall on distinct banks.
+constexpr int kPartStride = 67;
+
 struct FitterSmem {
-    float part[13 * 64];   // first-stage partial sums, 64 per batched value
+    float part[13 * kPartStride];   // first-stage partial sums of the batched values
     float out[16];         // reduction results
     float ucl;             // u[col] broadcast from its owner
     int status;            // nonzero: a bounded wait ran out
@@ -76,80 +82,115 @@ __device__ __forceinline__ float rop(float a, float b) {
     return fmax_cl(a, b);
 }
 
-// Batched work-group reduction of n <= VMAX values per thread.  Values
-// [0, split) use OP_A, [split, n) use OP_B (0 sum, 1 min, 2 max).  NMIN is a
-// compile-time lower bound on n: the guards of the values below it vanish.
-template <int VMAX, int OP_A, int OP_B, int NMIN = 0>
+// Batched work-group min/max reduction of n <= VMAX values per thread
+// (parallel_reduction_min/max, bmfr.cl:45-87).  Values [0, split) use OP_A,
+// [split, n) use OP_B (1 min, 2 max); results in sm.out.
+template <int VMAX, int OP_A, int OP_B>
 __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int split, FitterSmem& sm) {
+    static_assert(OP_A != 0 && OP_B != 0, "sums go through block_sum_dots or block_sum1_all");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (OP_A == 0 && OP_B == 0) {
-        // Sums, two values per packed add (bmfr.cl:33).
 #pragma unroll
-        for (int i = 0; i < VMAX; i += 2) {
-            if (i < NMIN || i < n) {
-                const float a0 = v[i], a1 = i + 1 < VMAX ? v[i + 1] : 0.0f;
-                const float2 a = make_float2(a0, a1);
-                const float2 b = make_float2(__shfl_down_sync(kFull, a0, 8), __shfl_down_sync(kFull, a1, 8));
-                const float2 c = make_float2(__shfl_down_sync(kFull, a0, 16), __shfl_down_sync(kFull, a1, 16));
-                const float2 d = make_float2(__shfl_down_sync(kFull, a0, 24), __shfl_down_sync(kFull, a1, 24));
-                const float2 s1 = __fadd2_rn(a, __fadd2_rn(__fadd2_rn(b, c), d));
-                if (lane < 8) {
-                    sm.part[i * 64 + 8 * warp + lane] = s1.x;
-                    if (i + 1 < NMIN || i + 1 < n) sm.part[(i + 1) * 64 + 8 * warp + lane] = s1.y;
-                }
-            }
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < VMAX; ++i) {
-            if (i < NMIN || i < n) {
-                const float a = v[i];
-                const float b = __shfl_down_sync(kFull, a, 8);
-                const float c = __shfl_down_sync(kFull, a, 16);
-                const float d = __shfl_down_sync(kFull, a, 24);
-                const int op = i < split ? OP_A : OP_B;
-                float s1;
-                if (op == 0) s1 = a + ((b + c) + d);                               // bmfr.cl:33
-                else if (op == 1) s1 = fmin_cl(fmin_cl(fmin_cl(a, b), c), d);    // bmfr.cl:52-53
-                else s1 = fmax_cl(fmax_cl(fmax_cl(a, b), c), d);                 // bmfr.cl:74-75
-                if (lane < 8) sm.part[i * 64 + 8 * warp + lane] = s1;
-            }
+    for (int i = 0; i < VMAX; ++i) {
+        if (i < n) {
+            const float a = v[i];
+            const float b = __shfl_down_sync(kFull, a, 8);
+            const float c = __shfl_down_sync(kFull, a, 16);
+            const float d = __shfl_down_sync(kFull, a, 24);
+            const int op = i < split ? OP_A : OP_B;
+            float s1;
+            if (op == 1) s1 = fmin_cl(fmin_cl(fmin_cl(a, b), c), d);    // bmfr.cl:52-53
+            else s1 = fmax_cl(fmax_cl(fmax_cl(a, b), c), d);            // bmfr.cl:74-75
+            if (lane < 8) sm.part[i * kPartStride + 8 * warp + lane] = s1;
         }
     }
     __syncthreads();
     // Stages 2 and 3: value vi is finished by the 8-lane group `lane >> 3` of
-    // warp vi % 8; lane j of the group forms sum_vec[j] (bmfr.cl:35-37).
+    // warp vi % 8; lane j of the group forms the j-th second-stage value
+    // (bmfr.cl:56-58), lane 0 of the group the result (bmfr.cl:60-63).
     const int vi = warp + 8 * (lane >> 3);
     const int j = lane & 7;
     const int op = vi < split ? OP_A : OP_B;
     float s2 = 0.0f;
     if (vi < n) {
-        const float* p = sm.part + vi * 64 + j;
-        if (op == 0) {
-            float acc = p[8];
+        const float* p = sm.part + vi * kPartStride + j;
+        float acc = p[0];
 #pragma unroll
-            for (int m = 2; m < 8; ++m) acc = acc + p[8 * m];
-            s2 = p[0] + acc;
-        } else {
-            float acc = p[0];
-#pragma unroll
-            for (int m = 1; m < 8; ++m) acc = op == 1 ? fmin_cl(acc, p[8 * m]) : fmax_cl(acc, p[8 * m]);
-            s2 = acc;
-        }
+        for (int m = 1; m < 8; ++m) acc = op == 1 ? fmin_cl(acc, p[8 * m]) : fmax_cl(acc, p[8 * m]);
+        s2 = acc;
     }
-    // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right,
-    // by lane 0 of the group from its lanes' values on shuffles.
     if (warp < n) {   // warp-uniform: warps without a value skip
         const int base = lane & ~7;
         float r = __shfl_sync(kFull, s2, base);
 #pragma unroll
         for (int m = 1; m < 8; ++m) {
             const float x = __shfl_sync(kFull, s2, base + m);
-            r = op == 0 ? r + x : (op == 1 ? fmin_cl(r, x) : fmax_cl(r, x));
+            r = op == 1 ? fmin_cl(r, x) : fmax_cl(r, x);
         }
         if (vi < n && j == 0) sm.out[vi] = r;
     }
     __syncthreads();
+}
+
+// parallel_reduction_sum (bmfr.cl:25-43) of the column step's n <= VMAX dot
+// products; results in sm.out.  NMIN is a compile-time lower bound on n: the
+// guards of the values below it vanish.  Returns, from the closing barrier,
+// whether any sum lies outside {0} and [2^-32, 2^30], the range in which the
+// update's quotients take Markstein's correction.
+//
+// Stage 1 (bmfr.cl:33) is a transposing exchange: the lanes of ids i+64 and
+// i+128 (groups 1 and 2) swap half of their values and form b + c, the lanes
+// of ids i and i+192 (groups 0 and 3) swap the other half and each receive
+// b + c from their neighbour group, so group 0 finishes values [0, H) and
+// group 3 values [H, 2H) as a + ((b + c) + d): one shuffle per value instead
+// of three.  Stages 2 and 3 as in block_reduce.
+template <int VMAX, int NMIN>
+__device__ __forceinline__ bool block_sum_dots(const float (&v)[VMAX], int n, FitterSmem& sm) {
+    constexpr int H = (VMAX + 1) / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 3;
+    const bool low = g < 2;   // groups 0 and 1 keep values [0, H), 2 and 3 values [H, 2H)
+    float* dst = sm.part + (g == 0 ? 0 : H * kPartStride) + 8 * warp + (lane & 7);
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        if (i < NMIN || i < n) {
+            const float x = v[i], y = H + i < VMAX ? v[H + i] : 0.0f;
+            const float keep = low ? x : y;
+            const float got = __shfl_xor_sync(kFull, low ? y : x, 24);
+            const float bc = keep + got;                            // groups 1 and 2: b + c
+            const float bc_in = __shfl_xor_sync(kFull, bc, 8);      // groups 0 and 3 receive it
+            const float a = g == 0 ? keep : got, d = g == 0 ? got : keep;
+            const float s1 = a + (bc_in + d);
+            if (g == 0 || (g == 3 && (H + i < NMIN || H + i < n))) dst[i * kPartStride] = s1;
+        }
+    }
+    __syncthreads();
+    // Stage 2 (bmfr.cl:35-37): value vi is finished by the 8-lane group
+    // `lane >> 3` of warp vi % 8; lane j of the group forms sum_vec[j].
+    const int vi = warp + 8 * g;
+    const int j = lane & 7;
+    float s2 = 0.0f;
+    if (vi < n) {
+        const float* p = sm.part + vi * kPartStride + j;
+        float acc = p[8];
+#pragma unroll
+        for (int m = 2; m < 8; ++m) acc = acc + p[8 * m];
+        s2 = p[0] + acc;
+    }
+    // Stage 3 (bmfr.cl:39-42): sum_vec[0] + ... + sum_vec[7], left to right,
+    // by lane 0 of the group from its lanes' values on shuffles.
+    bool out_of_range = false;
+    if (warp < n) {   // warp-uniform: warps without a value skip
+        const int base = lane & ~7;
+        float r = __shfl_sync(kFull, s2, base);
+#pragma unroll
+        for (int m = 1; m < 8; ++m) r = r + __shfl_sync(kFull, s2, base + m);
+        if (vi < n && j == 0) {
+            sm.out[vi] = r;
+            const float ar = fabsf(r);
+            out_of_range = !(ar == 0.0f || (ar >= 0x1p-32f && ar <= 0x1p30f));
+        }
+    }
+    return __syncthreads_or(out_of_range) != 0;
 }
 
 // parallel_reduction_sum (bmfr.cl:25-43) of one value per thread, finished by
@@ -157,9 +198,9 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
 // i+192), one barrier, then each warp reads the 64 first-stage sums and runs
 // stages 2 and 3 itself in the reference's order, so the sum reaches every
 // thread without a second barrier or a broadcast through shared memory.
-// part1 is rewritten only by the next call, and a batched block_reduce (two
-// barriers) separates consecutive calls in the column loop, so no warp can
-// overwrite sums another warp is still reading.
+// part1 is rewritten only by the next call, and block_sum_dots' barriers
+// separate consecutive calls in the column loop, so no warp can overwrite
+// sums another warp is still reading.
 __device__ __forceinline__ float block_sum1_all(float v, FitterSmem& sm) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float b = __shfl_down_sync(kFull, v, 8);
@@ -276,23 +317,30 @@ __device__ __forceinline__ void fill_noise_table(float* table, int frame) {
 // each rounded exactly as the scalar form, in one instruction.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-// Products that must round on their own: a packed multiply whose result
-// feeds a packed add is fused into one packed fused multiply-add by the
-// compiler (measured: the reference-arithmetic fitter then differed from the
-// reference in the last bits of most weights with float32 tmp_data, and of
-// ~1 % with binary16), while a scalar __fmul_rn is never contracted.  The
-// reference-arithmetic path and the noise term use these.
-__device__ __forceinline__ float2 rmul2(float2 a, float2 b) {
-    return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
-}
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// Products that must round on their own.  A packed multiply whose result
+// feeds a packed add is fused into one packed fused multiply-add by the
+// compiler, even when written in PTX with an explicit rounding mode
+// (measured: the reference-arithmetic fitter then differed from the
+// reference in the last bits of most weights with float32 tmp_data).  So the
+// product is a fused multiply-add with the addend nz = -0.0f, which the
+// caller reads at run time (NoiseConst::neg_zero): RN(a*b + -0) is RN(a*b)
+// with its sign of zero, and an FMA cannot be fused into the add it feeds.
+__device__ __forceinline__ float2 rmul2(float2 a, float2 b, float nz) { return __ffma2_rn(a, b, make_float2(nz, nz)); }
+// RN(a + c) for a binary16 a and a float c: the conversion of a is exact, so
+// this is the float addition of the reference, in one instruction.
+__device__ __forceinline__ float add_f32_h(__half a, float c) {
+    float d;
+    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(__half_as_ushort(a)), "f"(c));
+    return d;
+}
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 
 // add_noise_r on two values at once.
 __device__ __forceinline__ float2 add_noise_r2(float2 v, float2 r, NoiseConst c) {
     const float2 hi = dup2(c.hi), lo = dup2(c.lo);
-    const float2 p = rmul2(hi, r);
+    const float2 p = rmul2(hi, r, c.neg_zero);
     const float2 pe = fma2(hi, r, neg2(p));
     const float2 pl = fma2(lo, r, pe);
     const float2 sm = add2(v, p);
@@ -361,15 +409,15 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
             float2 a01, a23, b01, b23;
             load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
             load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
-            float2 s = add2(dup2(0.0f), rmul2(make_float2(a01.x, b01.x), uq0));
-            s = add2(s, rmul2(make_float2(a01.y, b01.y), uq1));
-            s = add2(s, rmul2(make_float2(a23.x, b23.x), uq2));
-            s = add2(s, rmul2(make_float2(a23.y, b23.y), uq3));
+            float2 s = add2(dup2(0.0f), rmul2(make_float2(a01.x, b01.x), uq0, nc.neg_zero));
+            s = add2(s, rmul2(make_float2(a01.y, b01.y), uq1, nc.neg_zero));
+            s = add2(s, rmul2(make_float2(a23.x, b23.x), uq2, nc.neg_zero));
+            s = add2(s, rmul2(make_float2(a23.y, b23.y), uq3, nc.neg_zero));
             d[i] = s.x;
             d[i + 1] = s.y;
         }
     }
-    block_reduce<VS, 0, 0, VMIN>(d, V, V, sm);
+    const bool dots_out = block_sum_dots<VS, VMIN>(d, V, sm);
 
     // Rank-one update, rounded at the reference's store (bmfr.cl:640-652).
     // Quotients take Markstein's correction when every operand is in range:
@@ -380,39 +428,78 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     const bool fast_b = uls >= 0x1p-60f && uls <= 0x1p60f;
     const float2 u2_01 = make_float2(2.0f * u0, 2.0f * c01.y), u2_23 = make_float2(2.0f * c23.x, 2.0f * c23.y);
     bool fast_u = fast_b;
-    {
+    if constexpr (HALF) {
+        // Finite binary16 values have |2u| = 0 or within [2^-23, 2^17]; only
+        // row `col` (the float ucl - vl) needs the full test.
+        const __half2 lim = __float2half2_rn(65504.0f);
+        const float m = fabsf(u2_01.x);
+        fast_u = fast_u && __hble2(__habs2(t.h[0][0]), lim) && __hble2(__habs2(t.h[0][1]), lim) &&
+                 (id != col || m == 0.0f || (m >= 0x1p-32f && m <= 0x1p30f));
+    } else {
         const float m[4] = {fabsf(u2_01.x), fabsf(u2_01.y), fabsf(u2_23.x), fabsf(u2_23.y)};
 #pragma unroll
         for (int q = 0; q < 4; ++q) fast_u = fast_u && (m[q] == 0.0f || (m[q] >= 0x1p-32f && m[q] <= 0x1p30f));
     }
     const float2 ny = dup2(-y), b2 = dup2(uls);
+    if (fast_u && !dots_out) {
+        // Every quotient of this thread in range (the common case).  The
+        // numerator and the first quotient estimate feed only multiplies and
+        // fused multiply-adds, never an add, so the packed multiply cannot be
+        // contracted here and rounds each lane as the reference's
+        // multiplication does.
 #pragma unroll
-    for (int i = 0; i < VS; ++i) {
-        if (i < VMIN || i < V) {
-            const float dot = sm.out[i];
-            const float ad = fabsf(dot);
-            const bool fast = fast_u && (ad == 0.0f || (ad >= 0x1p-32f && ad <= 0x1p30f));
-            float2 a01, a23;
-            load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
-            float2 n01, n23;
-            if (fast) {
-                // The numerator and the first quotient estimate feed only
-                // multiplies and fused multiply-adds, never an add, so the
-                // packed multiply cannot be contracted here and rounds each
-                // lane as the reference's multiplication does.
-                const float2 d2 = dup2(dot);
+        for (int i = 0; i < VS; ++i) {
+            if (i < VMIN || i < V) {
+                const float2 d2 = dup2(sm.out[i]);
                 const float2 num01 = mul2(u2_01, d2), num23 = mul2(u2_23, d2);
                 const float2 nq01 = mul2(num01, ny), nq23 = mul2(num23, ny);
                 const float2 r01 = fma2(nq01, b2, num01), r23 = fma2(nq23, b2, num23);
-                n01 = add2(a01, fma2(r01, ny, nq01));
-                n23 = add2(a23, fma2(r23, ny, nq23));
-            } else {
-                n01 = make_float2(a01.x - div_slow(u2_01.x * dot, uls), a01.y - div_slow(u2_01.y * dot, uls));
-                n23 = make_float2(a23.x - div_slow(u2_23.x * dot, uls), a23.y - div_slow(u2_23.y * dot, uls));
+                const float2 mq01 = fma2(r01, ny, nq01), mq23 = fma2(r23, ny, nq23);   // -RN(num / uls)
+                if constexpr (HALF && !NOISE) {
+                    // a - q straight from the binary16 a (add.f32.f16); row
+                    // id keeps its half when it lies above the column.
+                    const __half2 h01 = t.h[i + 1][0], h23 = t.h[i + 1][1];
+                    const __half2 n01 = __floats2half2_rn(add_f32_h(__low2half(h01), mq01.x),
+                                                          add_f32_h(__high2half(h01), mq01.y));
+                    t.h[i + 1][0] = row0 ? n01 : __halves2half2(__low2half(h01), __high2half(n01));
+                    t.h[i + 1][1] = __floats2half2_rn(add_f32_h(__low2half(h23), mq23.x),
+                                                      add_f32_h(__high2half(h23), mq23.y));
+                } else {
+                    float2 a01, a23;
+                    load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
+                    float2 n01 = add2(a01, mq01);
+                    const float2 n23 = add2(a23, mq23);
+                    if (!row0) n01.x = a01.x;
+                    t.set2(i + 1, 0, n01.x, n01.y);
+                    t.set2(i + 1, 1, n23.x, n23.y);
+                }
             }
-            if (!row0) n01.x = a01.x;
-            t.set2(i + 1, 0, n01.x, n01.y);
-            t.set2(i + 1, 1, n23.x, n23.y);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < VS; ++i) {
+            if (i < VMIN || i < V) {
+                const float dot = sm.out[i];
+                const float ad = fabsf(dot);
+                const bool fast = fast_u && (ad == 0.0f || (ad >= 0x1p-32f && ad <= 0x1p30f));
+                float2 a01, a23;
+                load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
+                float2 n01, n23;
+                if (fast) {
+                    const float2 d2 = dup2(dot);
+                    const float2 num01 = mul2(u2_01, d2), num23 = mul2(u2_23, d2);
+                    const float2 nq01 = mul2(num01, ny), nq23 = mul2(num23, ny);
+                    const float2 r01 = fma2(nq01, b2, num01), r23 = fma2(nq23, b2, num23);
+                    n01 = add2(a01, fma2(r01, ny, nq01));
+                    n23 = add2(a23, fma2(r23, ny, nq23));
+                } else {
+                    n01 = make_float2(a01.x - div_slow(u2_01.x * dot, uls), a01.y - div_slow(u2_01.y * dot, uls));
+                    n23 = make_float2(a23.x - div_slow(u2_23.x * dot, uls), a23.y - div_slow(u2_23.y * dot, uls));
+                }
+                if (!row0) n01.x = a01.x;
+                t.set2(i + 1, 0, n01.x, n01.y);
+                t.set2(i + 1, 1, n23.x, n23.y);
+            }
         }
     }
     t.shift();

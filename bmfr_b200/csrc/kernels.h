@@ -112,12 +112,13 @@ struct BlockJob {
 cudaError_t launch_fused_block(const Geometry& g, const AccumArgs& a, NoiseConst nc, float second_alpha,
                                int qr, bool half_history, const FusedBuffers& fb, bool pixels, cudaStream_t s);
 
-// NOISE_AMOUNT * 2 split into hi + lo floats.
+// NOISE_AMOUNT * 2 split into hi + lo floats, and the fitter's -0.0f.
 inline NoiseConst make_noise_const(double noise_amount) {
     const double c = noise_amount * 2.0;
     NoiseConst n;
     n.hi = (float)c;
     n.lo = (float)(c - (double)n.hi);
+    n.neg_zero = -0.0f;
     return n;
 }
 
