@@ -327,6 +327,14 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 // caller reads at run time (NoiseConst::neg_zero): RN(a*b + -0) is RN(a*b)
 // with its sign of zero, and an FMA cannot be fused into the add it feeds.
 __device__ __forceinline__ float2 rmul2(float2 a, float2 b, float nz) { return __ffma2_rn(a, b, make_float2(nz, nz)); }
+// RN(a*b + c) for binary16 a, b and a float c (fma.f32.f16): a*b is exact
+// in float, so this is RN(c + RN(a*b)), the reference's float multiply-add.
+__device__ __forceinline__ float fma_h(__half a, __half b, float c) {
+    float d;
+    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d)
+        : "h"(__half_as_ushort(a)), "h"(__half_as_ushort(b)), "f"(c));
+    return d;
+}
 // RN(a + c) for a binary16 a and a float c: the conversion of a is exact, so
 // this is the float addition of the reference, in one instruction.
 __device__ __forceinline__ float add_f32_h(__half a, float c) {
@@ -399,22 +407,58 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     // 0 + a*0 leaves the reference's partial sum 0 unchanged.
     const float2 uq0 = dup2(row0 ? u0 : 0.0f), uq1 = dup2(c01.y), uq2 = dup2(c23.x), uq3 = dup2(c23.y);
 
-    // Dot products with the later columns (bmfr.cl:606-638), two columns at
-    // a time in packed lanes; each lane keeps the reference's order.
+    // Dot products with the later columns (bmfr.cl:606-638): 0 + p0 + p1 +
+    // p2 + p3 in the reference's order for rows q0..q3.
     float d[VS];
+    if constexpr (HALF && !NOISE) {
+        // The product of two binary16 values is exact in float, so s + a*u
+        // rounds once either way and is one mixed-precision FMA.  Only the
+        // thread whose row q0 is row `col` (u = the float ucl - vl) forms
+        // that first product as a float product.
+        const __half u1 = __high2half(t.h[0][0]), u2 = __low2half(t.h[0][1]), u3 = __high2half(t.h[0][1]);
+        if (id != col) {
+            const __half u0 = id > col ? __low2half(t.h[0][0]) : __float2half(0.0f);   // 0 above the column
 #pragma unroll
-    for (int i = 0; i < VS; i += 2) {
-        d[i] = d[i + 1] = 0.0f;
-        if (i < VMIN || i < V) {
-            float2 a01, a23, b01, b23;
-            load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
-            load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
-            float2 s = add2(dup2(0.0f), rmul2(make_float2(a01.x, b01.x), uq0, nc.neg_zero));
-            s = add2(s, rmul2(make_float2(a01.y, b01.y), uq1, nc.neg_zero));
-            s = add2(s, rmul2(make_float2(a23.x, b23.x), uq2, nc.neg_zero));
-            s = add2(s, rmul2(make_float2(a23.y, b23.y), uq3, nc.neg_zero));
-            d[i] = s.x;
-            d[i + 1] = s.y;
+            for (int i = 0; i < VS; ++i) {
+                d[i] = 0.0f;
+                if (i < VMIN || i < V) d[i] = fma_h(__low2half(t.h[i + 1][0]), u0, 0.0f);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < VS; i += 2) {
+                d[i] = d[i + 1] = 0.0f;
+                if (i < VMIN || i < V) {
+                    const float2 a0 = make_float2(__low2float(t.h[i + 1][0]), __low2float(t.h[i + 2][0]));
+                    const float2 s = add2(dup2(0.0f), rmul2(a0, uq0, nc.neg_zero));
+                    d[i] = s.x;
+                    d[i + 1] = s.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < VS; ++i) {
+            if (i < VMIN || i < V) {
+                float s = fma_h(__high2half(t.h[i + 1][0]), u1, d[i]);
+                s = fma_h(__low2half(t.h[i + 1][1]), u2, s);
+                d[i] = fma_h(__high2half(t.h[i + 1][1]), u3, s);
+            }
+        }
+    } else {
+        // Two columns at a time in packed lanes; each lane keeps the order.
+#pragma unroll
+        for (int i = 0; i < VS; i += 2) {
+            d[i] = d[i + 1] = 0.0f;
+            if (i < VMIN || i < V) {
+                float2 a01, a23, b01, b23;
+                load_column<HALF, NOISE>(t, i + 1, i + 1, noise, nc, a01, a23);
+                load_column<HALF, NOISE>(t, i + 2, i + 2, noise, nc, b01, b23);
+                float2 s = add2(dup2(0.0f), rmul2(make_float2(a01.x, b01.x), uq0, nc.neg_zero));
+                s = add2(s, rmul2(make_float2(a01.y, b01.y), uq1, nc.neg_zero));
+                s = add2(s, rmul2(make_float2(a23.x, b23.x), uq2, nc.neg_zero));
+                s = add2(s, rmul2(make_float2(a23.y, b23.y), uq3, nc.neg_zero));
+                d[i] = s.x;
+                d[i + 1] = s.y;
+            }
         }
     }
     const bool dots_out = block_sum_dots<VS, VMIN>(d, V, sm);
