@@ -401,16 +401,16 @@ __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float ta
         rgb_to_ycocg(s, ycc);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const bool ok = in && ycc[c] == ycc[c];
-            const float vmn = ok ? ycc[c] : INFINITY, vmx = ok ? ycc[c] : -INFINITY;
+            // NaN and out-of-image entries as +-inf (fminf/fmaxf return the
+            // other operand of a NaN), so the neighbours' candidates come
+            // ready by shuffle; lanes 0 and 31, the halo columns, take their
+            // own as a neighbour and are not written.
+            const float vmn = in ? fminf(ycc[c], INFINITY) : INFINITY;
+            const float vmx = in ? fmaxf(ycc[c], -INFINITY) : -INFINITY;
             cmn[k][c] = vmn;
             cmx[k][c] = vmx;
-            const float l = __shfl_up_sync(0xffffffffu, ycc[c], 1), rr = __shfl_down_sync(0xffffffffu, ycc[c], 1);
-            const unsigned okm = __ballot_sync(0xffffffffu, ok);
-            const bool lok = lane > 0 && ((okm >> (lane - 1)) & 1u);
-            const bool rok = lane < 31 && ((okm >> (lane + 1)) & 1u);
-            hmn[k][c] = fminf(fminf(lok ? l : INFINITY, vmn), rok ? rr : INFINITY);
-            hmx[k][c] = fmaxf(fmaxf(lok ? l : -INFINITY, vmx), rok ? rr : -INFINITY);
+            hmn[k][c] = fminf(fminf(__shfl_up_sync(0xffffffffu, vmn, 1), vmn), __shfl_down_sync(0xffffffffu, vmn, 1));
+            hmx[k][c] = fmaxf(fmaxf(__shfl_up_sync(0xffffffffu, vmx, 1), vmx), __shfl_down_sync(0xffffffffu, vmx, 1));
         }
         if (r >= 2) {
             const int up = (r - 2) % 3, mid = (r - 1) % 3, dn = k;
