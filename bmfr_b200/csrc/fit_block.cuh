@@ -23,8 +23,9 @@
 // A column costs the norm (one barrier) and the dots (two) where the
 // reference spends three barriers per dot product.
 //
-// Columns run in a loop; after each column the register tile shifts down by
-// one column so that every index into it is a compile-time constant.
+// Columns run in a loop; each column's update writes later column k into
+// tile slot k - 1, so the tile moves down by one column as it is updated and
+// every index into it is a compile-time constant.
 //
 // Division.  The rank-one update divides by the column's |u|^2, which is the
 // same for the whole block.  Its correctly rounded reciprocal is formed once
@@ -119,11 +120,10 @@ __device__ __forceinline__ void block_reduce(const float (&v)[VMAX], int n, int 
         s2 = acc;
     }
     if (warp < n) {   // warp-uniform: warps without a value skip
-        const int base = lane & ~7;
-        float r = __shfl_sync(kFull, s2, base);
+        float r = __shfl_sync(kFull, s2, 0, 8);
 #pragma unroll
         for (int m = 1; m < 8; ++m) {
-            const float x = __shfl_sync(kFull, s2, base + m);
+            const float x = __shfl_sync(kFull, s2, m, 8);
             r = op == 1 ? fmin_cl(r, x) : fmax_cl(r, x);
         }
         if (vi < n && j == 0) sm.out[vi] = r;
@@ -180,10 +180,9 @@ __device__ __forceinline__ bool block_sum_dots(const float (&v)[VMAX], int n, Fi
     // by lane 0 of the group from its lanes' values on shuffles.
     bool out_of_range = false;
     if (warp < n) {   // warp-uniform: warps without a value skip
-        const int base = lane & ~7;
-        float r = __shfl_sync(kFull, s2, base);
+        float r = __shfl_sync(kFull, s2, 0, 8);
 #pragma unroll
-        for (int m = 1; m < 8; ++m) r = r + __shfl_sync(kFull, s2, base + m);
+        for (int m = 1; m < 8; ++m) r = r + __shfl_sync(kFull, s2, m, 8);
         if (vi < n && j == 0) {
             sm.out[vi] = r;
             const float ar = fabsf(r);
@@ -234,13 +233,6 @@ struct Tile<true> {   // binary16 storage: every store rounds to nearest even
     __half2 h[kBuffers][2];
     __device__ __forceinline__ float2 get2(int k, int p) const { return __half22float2(h[k][p]); }
     __device__ __forceinline__ void set2(int k, int p, float a, float b) { h[k][p] = __floats2half2_rn(a, b); }
-    __device__ __forceinline__ void shift() {
-#pragma unroll
-        for (int k = 0; k < kBuffers - 1; ++k) {
-            h[k][0] = h[k + 1][0];
-            h[k][1] = h[k + 1][1];
-        }
-    }
 };
 
 template <>
@@ -252,13 +244,6 @@ struct Tile<false> {   // float storage: no intermediate rounding; rows (q0,q1) 
     __device__ __forceinline__ void set1(int k, int q, float v) {
         if (q & 1) p[k][q >> 1].y = v;
         else p[k][q >> 1].x = v;
-    }
-    __device__ __forceinline__ void shift() {
-#pragma unroll
-        for (int k = 0; k < kBuffers - 1; ++k) {
-            p[k][0] = p[k + 1][0];
-            p[k][1] = p[k + 1][1];
-        }
     }
 };
 
@@ -372,8 +357,11 @@ __device__ __forceinline__ void load_column(const Tile<HALF>& t, int k, int fb, 
 }
 
 // One Householder column (bmfr.cl:549-655) on tile column 0; later columns
-// are tile columns 1..V.  NOISE: the first column, whose dot products read
-// features 1..9 with noise added (bmfr.cl:625-627).
+// are tile columns 1..V, and the update leaves later column k in tile
+// column k - 1, ready for the next column step (the slots beyond V hold
+// columns already finished and are never read again).  NOISE: the first
+// column, whose dot products read features 1..9 with noise added
+// (bmfr.cl:625-627).
 // VS: column slots the loops visit (a compile-time bound >= the V later
 // columns): the late columns take a shorter instance.  VMIN: a compile-time
 // bound <= V, so that the slots below it are visited without a guard.
@@ -505,8 +493,8 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
                     const __half2 h01 = t.h[i + 1][0], h23 = t.h[i + 1][1];
                     const __half2 n01 = __floats2half2_rn(add_f32_h(__low2half(h01), mq01.x),
                                                           add_f32_h(__high2half(h01), mq01.y));
-                    t.h[i + 1][0] = row0 ? n01 : __halves2half2(__low2half(h01), __high2half(n01));
-                    t.h[i + 1][1] = __floats2half2_rn(add_f32_h(__low2half(h23), mq23.x),
+                    t.h[i][0] = row0 ? n01 : __halves2half2(__low2half(h01), __high2half(n01));
+                    t.h[i][1] = __floats2half2_rn(add_f32_h(__low2half(h23), mq23.x),
                                                       add_f32_h(__high2half(h23), mq23.y));
                 } else {
                     float2 a01, a23;
@@ -514,8 +502,8 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
                     float2 n01 = add2(a01, mq01);
                     const float2 n23 = add2(a23, mq23);
                     if (!row0) n01.x = a01.x;
-                    t.set2(i + 1, 0, n01.x, n01.y);
-                    t.set2(i + 1, 1, n23.x, n23.y);
+                    t.set2(i, 0, n01.x, n01.y);
+                    t.set2(i, 1, n23.x, n23.y);
                 }
             }
         }
@@ -541,12 +529,11 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
                     n23 = make_float2(a23.x - div_slow(u2_23.x * dot, uls), a23.y - div_slow(u2_23.y * dot, uls));
                 }
                 if (!row0) n01.x = a01.x;
-                t.set2(i + 1, 0, n01.x, n01.y);
-                t.set2(i + 1, 1, n23.x, n23.y);
+                t.set2(i, 0, n01.x, n01.y);
+                t.set2(i, 1, n23.x, n23.y);
             }
         }
     }
-    t.shift();
 }
 
 // The precision form's fit (FP32 QR).  The same Householder reflections in
@@ -1004,7 +991,7 @@ __device__ __forceinline__ void fit_block(Tile<HALF>& t, const float* __restrict
         for (int col = 6; col < kFeatures; ++col) qr_column<HALF, false, 6, 3>(t, col, id, noise, nc, sm);   // 6..3
     }
 
-    // After ten shifts the colour columns are tile columns 0..2: rows 0..9
+    // After ten column steps the colour columns are tile columns 0..2: rows 0..9
     // form R's right-hand side (bmfr.cl:596-600 for col >= 10).
     if (id < kFeatures) {
         sm.rhs[id][0] = t.get2(0, 0).x;
