@@ -399,30 +399,25 @@ __device__ __forceinline__ void qr_column(Tile<HALF>& t, int col, int id, const 
     // p2 + p3 in the reference's order for rows q0..q3.
     float d[VS];
     if constexpr (HALF && !NOISE) {
-        // The product of two binary16 values is exact in float, so s + a*u
-        // rounds once either way and is one mixed-precision FMA.  Only the
-        // thread whose row q0 is row `col` (u = the float ucl - vl) forms
-        // that first product as a float product.
+        // Row q0 first, as a float product for every thread: the row `col`
+        // of one thread has the float u = ucl - vl, and a branch for that
+        // thread alone held its warp back at the next barrier (every warp
+        // doing the float products measured 4 % faster).  For the other
+        // rows a binary16 a times a binary16 u is exact in float, so there
+        // 0 + RN(a*u) is the same value the mixed FMA below would give.
         const __half u1 = __high2half(t.h[0][0]), u2 = __low2half(t.h[0][1]), u3 = __high2half(t.h[0][1]);
-        if (id != col) {
-            const __half u0 = id > col ? __low2half(t.h[0][0]) : __float2half(0.0f);   // 0 above the column
 #pragma unroll
-            for (int i = 0; i < VS; ++i) {
-                d[i] = 0.0f;
-                if (i < VMIN || i < V) d[i] = fma_h(__low2half(t.h[i + 1][0]), u0, 0.0f);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < VS; i += 2) {
-                d[i] = d[i + 1] = 0.0f;
-                if (i < VMIN || i < V) {
-                    const float2 a0 = make_float2(__low2float(t.h[i + 1][0]), __low2float(t.h[i + 2][0]));
-                    const float2 s = add2(dup2(0.0f), rmul2(a0, uq0, nc.neg_zero));
-                    d[i] = s.x;
-                    d[i + 1] = s.y;
-                }
+        for (int i = 0; i < VS; i += 2) {
+            d[i] = d[i + 1] = 0.0f;
+            if (i < VMIN || i < V) {
+                const float2 a0 = make_float2(__low2float(t.h[i + 1][0]), __low2float(t.h[i + 2][0]));
+                const float2 s = add2(dup2(0.0f), rmul2(a0, uq0, nc.neg_zero));
+                d[i] = s.x;
+                d[i + 1] = s.y;
             }
         }
+        // Rows q1..q3: a binary16 product is exact in float, so s + a*u
+        // rounds once either way and is one mixed-precision FMA.
 #pragma unroll
         for (int i = 0; i < VS; ++i) {
             if (i < VMIN || i < V) {
