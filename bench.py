@@ -98,11 +98,11 @@ def stage_bytes(w, h):
 # DRAM bytes (read + write) per launch at 1280x720 from one ncu capture of
 # the kernel (`bench.py --form probe --frames 6 --qr 0`, frame 3's launch;
 # profiles/k_fitter_720p.md, k_taa_720p.md).
-NCU_TRAFFIC_720P = {"fitter": 26.78e6, "taa": 25.95e6}
+NCU_TRAFFIC_720P = {"fitter": 26.78e6, "taa": 25.94e6}
 # Warp instructions per launch at 1280x720 (smsp__inst_executed.sum of the
 # same captures): the numerator of the issue-rate roofline of a kernel that
 # is bound by instruction issue rather than by HBM.
-NCU_WARP_INST_720P = {"fitter": 49.47e6, "taa": 12.67e6}
+NCU_WARP_INST_720P = {"fitter": 47.24e6, "taa": 11.43e6}
 SMS, SCHEDULERS_PER_SM = 148, 4
 # Kernels bound by instruction issue rather than by HBM or tensor cores.
 ISSUE_BOUND = {"fitter": "the fitter is a sequence of small dependent reductions and rank-one updates kept "
