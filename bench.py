@@ -346,7 +346,7 @@ def measure_batched(args, world, rank, local, dev, barrier, steps, warmup):
     fused: one graph-captured launch over all streams' blocks), binary16
     histories and FP32 QR (CholeskyQR2).  Beside it, the same streams one
     frame at a time through (a) the plain path (reference arithmetic, float
-    histories: the north star's baseline) and (b) plans with the batch's own
+    histories: the drop-in path the batched form is compared with) and (b) plans with the batch's own
     arithmetic and histories (the gain of batching alone).  Returns the
     measurement as a dict."""
     import torch
