@@ -56,6 +56,7 @@ struct FitterSmem {
     float Rm[10][10];      // R of the ten feature columns: Rm[x][y], y <= x
     float rhs[10][3];      // rows 0..9 of the three colour columns
     float part1[64];       // first-stage sums of block_sum1_all
+    float gram[88];        // CholeskyQR2: the Gram entries of a pass, summed over the warps
     float rowc[13];        // the precision form: row `col` of every column
     float inv1[10];        // CholeskyQR2: reciprocals of R1's and R2's diagonals,
     float inv2[10];        //   and the diagonal of the Gram matrix being factored
@@ -780,10 +781,23 @@ __device__ __forceinline__ void gram_all(const Tile<false>& t, FitterSmem& sm) {
     if constexpr (BASE + C < (PASS2 ? kGram2 : kGram1)) gram_all<C, PASS2, BASE + C>(t, sm);
 }
 
-// Warp 0, after the barrier that follows gram_chunk: lane j < 10 gathers
-// column j of the Gram matrix (g[i], i <= j; zeros below) and stores its
-// diagonal entry in diag[j]; lanes 10..12 gather the colour column
-// c = lane - 10 of the second pass; other lanes zeros.
+// After the barrier that follows gram_chunk: thread e sums Gram entry e over
+// the eight warps into sm.gram (85 threads at once, so warp 0's factorisation
+// starts from ten loads per lane instead of eighty).  A barrier follows.
+template <bool PASS2>
+__device__ __forceinline__ void gram_finish(FitterSmem& sm) {
+    const int e = threadIdx.x;
+    if (e < (PASS2 ? kGram2 : kGram1)) {
+        const float* p = sm.part + e;
+        sm.gram[e] = ((p[0] + p[kGramStride]) + (p[2 * kGramStride] + p[3 * kGramStride])) +
+                     ((p[4 * kGramStride] + p[5 * kGramStride]) + (p[6 * kGramStride] + p[7 * kGramStride]));
+    }
+}
+
+// Warp 0, after gram_finish and a barrier: lane j < 10 gathers column j of
+// the Gram matrix (g[i], i <= j; zeros below) and stores its diagonal entry
+// in diag[j]; lanes 10..12 gather the colour column c = lane - 10 of the
+// second pass; other lanes zeros.
 template <bool PASS2>
 __device__ __forceinline__ void gram_columns(FitterSmem& sm, int lane, float (&g)[kFeatures]) {
 #pragma unroll
@@ -791,12 +805,7 @@ __device__ __forceinline__ void gram_columns(FitterSmem& sm, int lane, float (&g
         int e = -1;
         if (lane < kFeatures) e = i <= lane ? lane * (lane + 1) / 2 + i : -1;
         else if (PASS2 && lane < kFeatures + 3) e = kGram1 + kFeatures * (lane - kFeatures) + i;
-        float s = 0.0f;
-        if (e >= 0) {
-            const float* p = sm.part + e;
-            s = ((p[0] + p[kGramStride]) + (p[2 * kGramStride] + p[3 * kGramStride])) +
-                ((p[4 * kGramStride] + p[5 * kGramStride]) + (p[6 * kGramStride] + p[7 * kGramStride]));
-        }
+        const float s = e >= 0 ? sm.gram[e] : 0.0f;
         g[i] = s;
         if (i == lane) sm.diag[i] = s;
     }
@@ -843,6 +852,8 @@ __device__ __forceinline__ void fit_columns_cqr2(Tile<false>& t, const float* __
     // Pass 1: R1 = chol(A^T A).
     gram_all<kGramChunk, false>(t, sm);
     __syncthreads();
+    gram_finish<false>(sm);
+    __syncthreads();
     if (warp == 0) {
         float g[kFeatures];
         gram_columns<false>(sm, lane, g);
@@ -870,6 +881,8 @@ __device__ __forceinline__ void fit_columns_cqr2(Tile<false>& t, const float* __
     }
     // Pass 2: R2 = chol(Q1^T Q1) and z = R2^-T Q1^T B.
     gram_all<kGramChunk, true>(t, sm);
+    __syncthreads();
+    gram_finish<true>(sm);
     __syncthreads();
     if (warp == 0) {
         float g[kFeatures];
