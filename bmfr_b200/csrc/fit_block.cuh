@@ -817,16 +817,22 @@ __device__ __forceinline__ void gram_columns(FitterSmem& sm, int lane, float (&g
 // its diagonal.  Out: lane j holds column j of R (g[i] = R(i, j)), lanes
 // 10..12 hold R^-T times their column, and inv[k] = 1 / R(k, k) (0 for a
 // dependent column) in shared memory.
+// The next pivot, lane k+1's g[k+1] after step k, is formed from that lane's
+// own registers and broadcast before the step's other shuffles, so the
+// chain of pivots does not wait for them (the same fused multiply-add the
+// update below performs in that lane).
 __device__ __forceinline__ void chol_lanes(float (&g)[kFeatures], int lane, const float* diag, float* inv) {
+    float dnext = __shfl_sync(kFull, g[0], 0);
 #pragma unroll
     for (int k = 0; k < kFeatures; ++k) {
-        const float d = __shfl_sync(kFull, g[k], k);
+        const float d = dnext;
         const bool ok = d > 0x1p-20f * diag[k];
         const float y = ok ? rsqrtf(d) : 0.0f;   // 1 / R(k, k)
         const float r = d * y;
         if (lane == 0) inv[k] = y;
         if (lane == k) g[k] = r;
         else if (lane > k) g[k] = g[k] * y;
+        if (k + 1 < kFeatures) dnext = __shfl_sync(kFull, __fmaf_rn(-g[k], g[k], g[k + 1]), k + 1);
 #pragma unroll
         for (int i = 0; i < kFeatures; ++i) {
             if (i > k) {
