@@ -185,6 +185,33 @@ class Plan:
         check(lib.bmfr_denoise_frame_io(self.handle, C.byref(io), mp, op, _stream_ptr(stream)),
               "bmfr_denoise_frame_io")
 
+    def denoise_frames(self, frames, prev_frame_camera_matrices, pixel_offsets, stream=None) -> None:
+        """Consecutive frames in one call (bmfr_denoise_frames): `frames` is a
+        sequence of dicts with the keys of denoise_frame_io's buffers
+        (albedo, normals, positions, noisy, previous_normals,
+        previous_positions, optional result), one camera matrix and pixel
+        offset per frame.  Outputs equal those of one denoise_frame_io call per
+        frame; the staged pipeline overlaps each frame's accumulation with the
+        previous frame's later stages."""
+        count = len(frames)
+        n = self.width * self.height * 12
+        first = self.frame_number
+        ios = (FrameIO * max(count, 1))()
+        for k, fr in enumerate(frames):
+            at0 = first + k == 0
+            ios[k] = FrameIO(_ptr(fr["albedo"], "albedo", n), _ptr(fr["normals"], "normals", n),
+                             _ptr(fr["positions"], "positions", n), _ptr(fr["noisy"], "noisy", n),
+                             _ptr(fr.get("previous_normals"), "previous_normals", n, optional=at0),
+                             _ptr(fr.get("previous_positions"), "previous_positions", n, optional=at0),
+                             _ptr(fr.get("result"), "result", n, optional=True))
+        mats = np.ascontiguousarray(np.asarray(prev_frame_camera_matrices, dtype=np.float32).reshape(-1))
+        offs = np.ascontiguousarray(np.asarray(pixel_offsets, dtype=np.float32).reshape(-1))
+        if mats.size != 16 * count or offs.size != 2 * count:
+            raise ValueError(f"{count} camera matrices (16 floats) and pixel offsets (2 floats) expected")
+        fp = C.POINTER(C.c_float)
+        check(lib.bmfr_denoise_frames(self.handle, count, ios, mats.ctypes.data_as(fp), offs.ctypes.data_as(fp),
+                                      _stream_ptr(stream)), "bmfr_denoise_frames")
+
     def result_ptr(self) -> int:
         p = C.c_void_p()
         check(lib.bmfr_plan_result(self.handle, C.byref(p)), "bmfr_plan_result")

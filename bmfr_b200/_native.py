@@ -125,6 +125,7 @@ def _load() -> C.CDLL:
         "bmfr_plan_upload_frame": (i, [vp, vp, vp, vp, vp, vp]),
         "bmfr_denoise_frame": (i, [vp, fp, fp, vp]),
         "bmfr_denoise_frame_io": (i, [vp, C.POINTER(FrameIO), fp, fp, vp]),
+        "bmfr_denoise_frames": (i, [vp, i, C.POINTER(FrameIO), fp, fp, vp]),
         "bmfr_plan_result": (i, [vp, C.POINTER(vp)]),
         "bmfr_plan_download_result": (i, [vp, vp, vp]),
         "bmfr_plan_frame_number": (i, [vp]),

@@ -48,18 +48,25 @@ struct bmfr_plan {
     float* noisy_in[3] = {nullptr, nullptr, nullptr};   // the frame's 1-spp colour
     void* noisy_acc[2] = {nullptr, nullptr};    // accumulated noisy history
     uint8_t* spp[2] = {nullptr, nullptr};
-    void* tmp = nullptr;
+    // Per-frame buffers that the accumulation writes and only the same
+    // frame's later stages read.  Set 1 exists once bmfr_denoise_frames has
+    // overlapped frames (frame f then uses set f & 1); otherwise every frame
+    // uses set 0.
+    struct FrameScratch {
+        void* tmp = nullptr;
+        float2* prev_pix = nullptr;
+        uint8_t* accept = nullptr;
+        float* noise_table = nullptr;   // the frame's fitter noise
+    } scratch[2];
+    int last_set = 0;                   // the set of the last frame
     float* weights = nullptr;
     float* mins_maxs = nullptr;
     float* filtered = nullptr;
-    float2* prev_pix = nullptr;
-    uint8_t* accept = nullptr;
     float* tone_mapped = nullptr;
     void* acc_filt[2] = {nullptr, nullptr};     // accumulated filtered history
     void* result[2] = {nullptr, nullptr};       // TAA history
     float* result_f32[2] = {nullptr, nullptr};  // fp32 output when histories are binary16
     int* dev_status = nullptr;                  // device error word (bounded waits)
-    float* noise_table = nullptr;               // the frame's fitter noise (scratch)
     const float* last_result = nullptr;         // float32 output of the last frame
     bool profiling = false;
     bool profiled_frame = false;
@@ -70,6 +77,11 @@ struct bmfr_plan {
     // parity p read back.  The flags say whether the event was recorded.
     cudaEvent_t ev_uploaded[3] = {}, ev_frame_done[3] = {}, ev_downloaded[2] = {};
     bool uploaded[3] = {}, downloaded[2] = {}, done_recorded[3] = {};
+    // bmfr_denoise_frames: the stream that runs the accumulations of
+    // overlapped frames, the end of frame f's accumulation (index f & 1) and
+    // the call's entry point on the caller's stream.
+    cudaStream_t acc_stream = nullptr;
+    cudaEvent_t ev_accumulated[2] = {}, ev_entry = nullptr;
     std::vector<void*> allocations;
 };
 
@@ -117,6 +129,10 @@ void free_plan(bmfr_plan* plan) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : plan->ev_downloaded)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : plan->ev_accumulated)
+        if (e) cudaEventDestroy(e);
+    if (plan->ev_entry) cudaEventDestroy(plan->ev_entry);
+    if (plan->acc_stream) cudaStreamDestroy(plan->acc_stream);
     for (void* p : plan->allocations) cudaFree(p);
     delete plan;
 }
@@ -237,12 +253,13 @@ int bmfr_plan_create(const bmfr_params* params, int width, int height, bmfr_plan
              alloc(pixel3_bytes(plan, half_hist), &plan->result[i]);
         if (ok && half_hist) ok = alloc(px * 12, &plan->result_f32[i]);
     }
-    ok = ok && alloc(tmp_bytes(g, half_tmp), &plan->tmp) &&
+    bmfr_plan::FrameScratch& fs = plan->scratch[0];
+    ok = ok && alloc(tmp_bytes(g, half_tmp), &fs.tmp) &&
          alloc((size_t)g.blocks * bmfr::kFeatures * 3 * 4, &plan->weights) &&
          alloc((size_t)g.blocks * bmfr::kScaled * 2 * 4, &plan->mins_maxs) &&
-         alloc(px * 12, &plan->filtered) && alloc(px * 8, &plan->prev_pix) && alloc(px, &plan->accept) &&
+         alloc(px * 12, &plan->filtered) && alloc(px * 8, &fs.prev_pix) && alloc(px, &fs.accept) &&
          alloc(px * 12, &plan->tone_mapped);
-    if (ok) ok = alloc(sizeof(int), &plan->dev_status) && alloc(bmfr::kNoiseTableBytes, &plan->noise_table);
+    if (ok) ok = alloc(sizeof(int), &plan->dev_status) && alloc(bmfr::kNoiseTableBytes, &fs.noise_table);
     for (int i = 0; i < 3 && ok; ++i)
         ok = cudaEventCreateWithFlags(&plan->ev_uploaded[i], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&plan->ev_frame_done[i], cudaEventDisableTiming) == cudaSuccess;
@@ -467,27 +484,35 @@ int bmfr_plan_upload_frame(bmfr_plan* plan, const float* albedo, const float* no
 namespace {
 
 // One frame of the pipeline (bmfr.cpp:429-476) on the given inputs; the
-// histories are the plan's.  prev_n/prev_p may be null at frame 0.
+// histories are the plan's.  prev_n/prev_p may be null at frame 0.  The
+// frame's noise table and accumulation run on `sa` (the plan's accumulation
+// stream while bmfr_denoise_frames overlaps frames, else `s`) into per-frame
+// buffer set `set`; everything after them runs on `s`.
 int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const float* prev_n, const float* cur_p,
               const float* prev_p, const float* noisy, float* extra_result, const float* m, const float* off,
-              cudaStream_t s) {
+              cudaStream_t s, cudaStream_t sa = nullptr, int set = 0) {
     const int f = plan->frame;
     const int cur = f & 1, prv = cur ^ 1;
     const bmfr::Geometry& g = plan->g;
     const bool half_tmp = plan->p.use_half_precision_in_tmp_data != 0;
     const bool half_hist = plan->p.half_history != 0;
+    // The fused pipeline accumulates inside its block kernel: never split.
+    const bool split = sa != nullptr && sa != s && plan->p.pipeline == BMFR_PIPELINE_STAGED;
+    if (!split) sa = s;
+    const bmfr_plan::FrameScratch& fs = plan->scratch[set];
     if (f > 0 && (!prev_n || !prev_p)) return fail(BMFR_E_INVALID, "denoise_frame: previous G-buffer missing");
     const bmfr::AccumArgs a = accum_args(plan, m, off, f);
-    const bool prof = plan->profiling;
+    const bool prof = plan->profiling && !split;
     auto mark = [&](int i) {
         if (prof) cudaEventRecord(plan->events[i], s);
     };
     cudaError_t e = cudaSuccess;
     // Uploads and downloads may run on other streams: wait for this frame's
-    // input set and for the read-back of the result buffers this frame
-    // overwrites (those of frame f-2).
+    // input set (read first by the accumulation; the later stages are
+    // ordered after it) and for the read-back of the result buffers this
+    // frame overwrites (those of frame f-2).
     if (plan->uploaded[f % 3] && albedo == plan->albedo[f % 3]) {
-        e = cudaStreamWaitEvent(s, plan->ev_uploaded[f % 3], 0);
+        e = cudaStreamWaitEvent(sa, plan->ev_uploaded[f % 3], 0);
         plan->uploaded[f % 3] = false;
     }
     if (e == cudaSuccess && plan->downloaded[cur]) {
@@ -495,7 +520,7 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         plan->downloaded[cur] = false;
     }
     mark(0);
-    if (e == cudaSuccess) e = bmfr::launch_noise_table(f, plan->noise_table, s);
+    if (e == cudaSuccess) e = bmfr::launch_noise_table(f, fs.noise_table, sa);
     if (plan->p.pipeline == BMFR_PIPELINE_FUSED) {
         mark(1);
         bmfr::FusedBuffers fb;
@@ -509,27 +534,30 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
         fb.noisy_acc_prev = plan->noisy_acc[prv];
         fb.prev_spp = plan->spp[prv];
         fb.cur_spp = plan->spp[cur];
-        fb.prev_pix = plan->prev_pix;
-        fb.accept = plan->accept;
+        fb.prev_pix = fs.prev_pix;
+        fb.accept = fs.accept;
         fb.tone_mapped = plan->tone_mapped;
         fb.acc_prev = plan->acc_filt[prv];
         fb.acc_cur = plan->acc_filt[cur];
         fb.weights = plan->weights;
         fb.mins_maxs = plan->mins_maxs;
-        fb.noise = plan->noise_table;
+        fb.noise = fs.noise_table;
         if (e == cudaSuccess)
             e = bmfr::launch_fused_block(g, a, bmfr::make_noise_const(plan->p.noise_amount),
                                          plan->p.second_blend_alpha, plan->p.fp32_qr, half_hist, fb, false, s);
         mark(2);
     } else {
         if (e == cudaSuccess)
-            e = bmfr::launch_accumulate_noisy(g, a, plan->prev_pix, plan->accept, cur_n, prev_n, cur_p, prev_p,
-                                              noisy, plan->noisy_acc[cur], plan->noisy_acc[prv], half_hist,
-                                              plan->spp[prv], plan->spp[cur], plan->tmp, s);
+            e = bmfr::launch_accumulate_noisy(g, a, fs.prev_pix, fs.accept, cur_n, prev_n, cur_p, prev_p, noisy,
+                                              plan->noisy_acc[cur], plan->noisy_acc[prv], half_hist, plan->spp[prv],
+                                              plan->spp[cur], fs.tmp, sa);
         mark(1);
+        // The rest of the frame waits for its accumulation only.
+        if (e == cudaSuccess && split) e = cudaEventRecord(plan->ev_accumulated[cur], sa);
+        if (e == cudaSuccess && split) e = cudaStreamWaitEvent(s, plan->ev_accumulated[cur], 0);
         if (e == cudaSuccess)
-            e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), plan->tmp, half_tmp,
-                                    plan->p.fp32_qr, plan->weights, plan->mins_maxs, plan->noise_table,
+            e = bmfr::launch_fitter(g, f, bmfr::make_noise_const(plan->p.noise_amount), fs.tmp, half_tmp,
+                                    plan->p.fp32_qr, plan->weights, plan->mins_maxs, fs.noise_table,
                                     plan->dev_status, s);
         mark(2);
     }
@@ -539,22 +567,56 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     if (e == cudaSuccess)
         e = bmfr::launch_weighted_sum_accumulate(g, f, plan->p.second_blend_alpha, plan->weights, plan->mins_maxs,
                                                  cur_n, cur_p, plan->keep_intermediates ? plan->filtered : nullptr,
-                                                 plan->prev_pix, plan->accept, albedo, plan->tone_mapped,
+                                                 fs.prev_pix, fs.accept, albedo, plan->tone_mapped,
                                                  plan->spp[cur], plan->acc_filt[prv], plan->acc_filt[cur], half_hist,
                                                  s);
     mark(3);
     mark(4);
     float* f32_out = extra_result ? extra_result : (half_hist ? plan->result_f32[cur] : nullptr);
     if (e == cudaSuccess)
-        e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, plan->prev_pix, plan->tone_mapped, plan->result[cur],
+        e = bmfr::launch_taa(g, f, plan->p.taa_blend_alpha, fs.prev_pix, plan->tone_mapped, plan->result[cur],
                              plan->result[prv], f32_out, half_hist, s);
     mark(5);
     if (e == cudaSuccess) e = cudaEventRecord(plan->ev_frame_done[f % 3], s);
     if (e != cudaSuccess) return cuda_fail(e, "denoise_frame launch");
     plan->done_recorded[f % 3] = true;
     plan->profiled_frame = prof;
+    plan->last_set = set;
     plan->last_result = half_hist ? f32_out : (const float*)plan->result[cur];
     plan->frame = f + 1;   // swaps every double buffer (bmfr.cpp:482-484)
+    return BMFR_OK;
+}
+
+// The second set of per-frame buffers, the accumulation stream and its
+// events, made by the first call that overlaps frames.  Set 1 is published
+// only when all of it exists.
+int ensure_overlap_resources(bmfr_plan* plan, cudaStream_t s) {
+    if (plan->scratch[1].tmp) return BMFR_OK;
+    const size_t px = (size_t)plan->g.W * plan->g.H;
+    bmfr_plan::FrameScratch fs;
+    const size_t bytes[4] = {tmp_bytes(plan->g, plan->p.use_half_precision_in_tmp_data != 0), px * 8, px,
+                             bmfr::kNoiseTableBytes};
+    void* ptr[4] = {};
+    for (int i = 0; i < 4; ++i) {
+        if (cudaMalloc(&ptr[i], bytes[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(BMFR_E_NOMEM, "device allocation for overlapped frames failed");
+        }
+        plan->allocations.push_back(ptr[i]);
+        cudaError_t e = cudaMemsetAsync(ptr[i], 0, bytes[i], s);
+        if (e != cudaSuccess) return cuda_fail(e, "overlapped frames: buffer initialisation");
+    }
+    cudaError_t e = cudaSuccess;
+    if (!plan->acc_stream) e = cudaStreamCreateWithFlags(&plan->acc_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+        if (!plan->ev_accumulated[i]) e = cudaEventCreateWithFlags(&plan->ev_accumulated[i], cudaEventDisableTiming);
+    if (e == cudaSuccess && !plan->ev_entry) e = cudaEventCreateWithFlags(&plan->ev_entry, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "overlapped frames: stream and events");
+    fs.tmp = ptr[0];
+    fs.prev_pix = static_cast<float2*>(ptr[1]);
+    fs.accept = static_cast<uint8_t*>(ptr[2]);
+    fs.noise_table = static_cast<float*>(ptr[3]);
+    plan->scratch[1] = fs;
     return BMFR_OK;
 }
 
@@ -579,6 +641,51 @@ int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io, const float*
         return fail(BMFR_E_INVALID, "denoise_frame_io: NULL input buffer");
     return run_frame(plan, io->albedo, io->normals, io->previous_normals, io->positions, io->previous_positions,
                      io->noisy, io->result, prev_frame_camera_matrix, pixel_offset, (cudaStream_t)stream);
+}
+
+int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io, const float* prev_frame_camera_matrices,
+                        const float* pixel_offsets, void* stream) {
+    if (int st = check_plan(plan)) return st;
+    if (count < 0) return fail(BMFR_E_INVALID, "denoise_frames: negative count");
+    if (count == 0) return BMFR_OK;
+    if (!io || !prev_frame_camera_matrices || !pixel_offsets)
+        return fail(BMFR_E_INVALID, "denoise_frames: NULL argument");
+    // Every frame is checked before the first is queued, so a bad entry
+    // leaves the plan where it was.
+    for (int i = 0; i < count; ++i) {
+        const bmfr_frame_io& x = io[i];
+        if (!x.albedo || !x.normals || !x.positions || !x.noisy)
+            return fail(BMFR_E_INVALID, "denoise_frames: NULL input buffer in io[" + std::to_string(i) + "]");
+        if (plan->frame + i > 0 && (!x.previous_normals || !x.previous_positions))
+            return fail(BMFR_E_INVALID, "denoise_frames: previous G-buffer missing in io[" + std::to_string(i) + "]");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool overlap = count > 1 && plan->p.pipeline == BMFR_PIPELINE_STAGED && !plan->profiling;
+    cudaStream_t sa = nullptr;
+    if (overlap) {
+        if (int st = ensure_overlap_resources(plan, s)) return st;
+        sa = plan->acc_stream;
+        // The accumulation stream starts after the work already on `stream`.
+        cudaError_t e = cudaEventRecord(plan->ev_entry, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sa, plan->ev_entry, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: entry");
+    }
+    for (int i = 0; i < count; ++i) {
+        const bmfr_frame_io& x = io[i];
+        const int f = plan->frame;
+        // Frame f's accumulation rewrites the per-frame buffers and the spp
+        // history that frame f-2 read on `stream`; frame f-1 uses the other
+        // set, and its accumulation precedes this one on the same stream.
+        if (overlap && i >= 2) {
+            cudaError_t e = cudaStreamWaitEvent(sa, plan->ev_frame_done[(f - 2) % 3], 0);
+            if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: frame order");
+        }
+        if (int st = run_frame(plan, x.albedo, x.normals, x.previous_normals, x.positions, x.previous_positions,
+                               x.noisy, x.result, prev_frame_camera_matrices + 16 * (size_t)i,
+                               pixel_offsets + 2 * (size_t)i, s, sa, overlap ? (f & 1) : 0))
+            return st;
+    }
+    return BMFR_OK;
 }
 
 int bmfr_plan_result(const bmfr_plan* plan, const float** result) {
@@ -671,13 +778,14 @@ int bmfr_plan_buffers_get(const bmfr_plan* plan, bmfr_plan_buffers* b) {
     std::memset(b, 0, sizeof *b);
     const int last = (plan->frame + 1) & 1;   // slot written by the last frame
     const bool staged = plan->p.pipeline == BMFR_PIPELINE_STAGED;
-    b->tmp_data = staged ? plan->tmp : nullptr;   // the fused pipeline keeps tmp_data on chip
+    const bmfr_plan::FrameScratch& fs = plan->scratch[plan->last_set];
+    b->tmp_data = staged ? fs.tmp : nullptr;   // the fused pipeline keeps tmp_data on chip
     b->weights = plan->weights;
     b->mins_maxs = plan->mins_maxs;
     b->filtered = plan->keep_intermediates ? plan->filtered : nullptr;
-    b->prev_frame_pixel = reinterpret_cast<const float*>(plan->prev_pix);
+    b->prev_frame_pixel = reinterpret_cast<const float*>(fs.prev_pix);
     b->tone_mapped = plan->tone_mapped;
-    b->accept = plan->accept;
+    b->accept = fs.accept;
     b->spp = plan->spp[last];
     b->accumulated_noisy = plan->noisy_acc[last];
     b->accumulated_filtered = plan->acc_filt[last];
