@@ -77,11 +77,12 @@ struct bmfr_plan {
     // parity p read back.  The flags say whether the event was recorded.
     cudaEvent_t ev_uploaded[3] = {}, ev_frame_done[3] = {}, ev_downloaded[2] = {};
     bool uploaded[3] = {}, downloaded[2] = {}, done_recorded[3] = {};
-    // bmfr_denoise_frames: the stream that runs the accumulations of
-    // overlapped frames, the end of frame f's accumulation (index f & 1) and
-    // the call's entry point on the caller's stream.
-    cudaStream_t acc_stream = nullptr;
-    cudaEvent_t ev_accumulated[2] = {}, ev_entry = nullptr;
+    // bmfr_denoise_frames: the streams that run the accumulations of
+    // overlapped frames (lowest priority) and the rest of each frame
+    // (highest priority), the end of frame f's accumulation (index f & 1),
+    // and the call's entry and exit on the caller's stream.
+    cudaStream_t acc_stream = nullptr, frame_stream = nullptr;
+    cudaEvent_t ev_accumulated[2] = {}, ev_entry = nullptr, ev_exit = nullptr;
     std::vector<void*> allocations;
 };
 
@@ -132,7 +133,9 @@ void free_plan(bmfr_plan* plan) {
     for (cudaEvent_t& e : plan->ev_accumulated)
         if (e) cudaEventDestroy(e);
     if (plan->ev_entry) cudaEventDestroy(plan->ev_entry);
+    if (plan->ev_exit) cudaEventDestroy(plan->ev_exit);
     if (plan->acc_stream) cudaStreamDestroy(plan->acc_stream);
+    if (plan->frame_stream) cudaStreamDestroy(plan->frame_stream);
     for (void* p : plan->allocations) cudaFree(p);
     delete plan;
 }
@@ -587,9 +590,13 @@ int run_frame(bmfr_plan* plan, const float* albedo, const float* cur_n, const fl
     return BMFR_OK;
 }
 
-// The second set of per-frame buffers, the accumulation stream and its
-// events, made by the first call that overlaps frames.  Set 1 is published
-// only when all of it exists.
+// The second set of per-frame buffers, the two streams and their events,
+// made by the first call that overlaps frames.  Set 1 is published only when
+// all of it exists.  The accumulation of frame f+1 has the length of frame
+// f's later stages as slack, so its stream has the lowest priority and the
+// other the highest: the block scheduler then gives free SM slots to the
+// fitter, weighted sum and TAA first, and the accumulation takes the slots
+// they leave (mostly in the fitter's last wave).
 int ensure_overlap_resources(bmfr_plan* plan, cudaStream_t s) {
     if (plan->scratch[1].tmp) return BMFR_OK;
     const size_t px = (size_t)plan->g.W * plan->g.H;
@@ -606,11 +613,16 @@ int ensure_overlap_resources(bmfr_plan* plan, cudaStream_t s) {
         cudaError_t e = cudaMemsetAsync(ptr[i], 0, bytes[i], s);
         if (e != cudaSuccess) return cuda_fail(e, "overlapped frames: buffer initialisation");
     }
-    cudaError_t e = cudaSuccess;
-    if (!plan->acc_stream) e = cudaStreamCreateWithFlags(&plan->acc_stream, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess && !plan->acc_stream)
+        e = cudaStreamCreateWithPriority(&plan->acc_stream, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess && !plan->frame_stream)
+        e = cudaStreamCreateWithPriority(&plan->frame_stream, cudaStreamNonBlocking, greatest);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i)
         if (!plan->ev_accumulated[i]) e = cudaEventCreateWithFlags(&plan->ev_accumulated[i], cudaEventDisableTiming);
     if (e == cudaSuccess && !plan->ev_entry) e = cudaEventCreateWithFlags(&plan->ev_entry, cudaEventDisableTiming);
+    if (e == cudaSuccess && !plan->ev_exit) e = cudaEventCreateWithFlags(&plan->ev_exit, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "overlapped frames: stream and events");
     fs.tmp = ptr[0];
     fs.prev_pix = static_cast<float2*>(ptr[1]);
@@ -659,15 +671,17 @@ int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io, con
         if (plan->frame + i > 0 && (!x.previous_normals || !x.previous_positions))
             return fail(BMFR_E_INVALID, "denoise_frames: previous G-buffer missing in io[" + std::to_string(i) + "]");
     }
-    cudaStream_t s = (cudaStream_t)stream;
+    cudaStream_t caller = (cudaStream_t)stream, s = caller;
     const bool overlap = count > 1 && plan->p.pipeline == BMFR_PIPELINE_STAGED && !plan->profiling;
     cudaStream_t sa = nullptr;
     if (overlap) {
-        if (int st = ensure_overlap_resources(plan, s)) return st;
+        if (int st = ensure_overlap_resources(plan, caller)) return st;
         sa = plan->acc_stream;
-        // The accumulation stream starts after the work already on `stream`.
-        cudaError_t e = cudaEventRecord(plan->ev_entry, s);
+        s = plan->frame_stream;
+        // Both streams start after the work already on the caller's stream.
+        cudaError_t e = cudaEventRecord(plan->ev_entry, caller);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(sa, plan->ev_entry, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, plan->ev_entry, 0);
         if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: entry");
     }
     for (int i = 0; i < count; ++i) {
@@ -684,6 +698,13 @@ int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io, con
                                x.noisy, x.result, prev_frame_camera_matrices + 16 * (size_t)i,
                                pixel_offsets + 2 * (size_t)i, s, sa, overlap ? (f & 1) : 0))
             return st;
+    }
+    if (overlap) {
+        // Every accumulation has been waited for on the frame stream; its
+        // last TAA ends the call on the caller's stream.
+        cudaError_t e = cudaEventRecord(plan->ev_exit, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, plan->ev_exit, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: exit");
     }
     return BMFR_OK;
 }

@@ -277,14 +277,16 @@ int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io,
  * call is ordered after the work already on `stream`, and work queued on
  * `stream` after it sees every frame's output (io[i].result where given; the
  * last frame's through bmfr_plan_result).  With the staged pipeline the
- * accumulation of frame i+1 runs on a stream of the plan's own while frame
- * i's fitter, weighted sum and TAA run on `stream`: the accumulation only
- * needs frame i's accumulated history, and the plan alternates two sets of
- * the per-frame buffers it writes (tmp_data, reprojected positions, accept
- * mask, fitter noise table).  The first such call allocates that second set
- * (about 40 B per pixel).  The buffers io[] points to must not be written
- * while the call's work runs.  The fused pipeline, and any call while stage
- * profiling is on, runs the frames one after another on `stream`. */
+ * accumulation of frame i+1 runs while frame i's fitter, weighted sum and
+ * TAA run, on two streams of the plan's own (the accumulation at the
+ * device's lowest stream priority, the rest at its highest) forked from and
+ * joined back into `stream`: the accumulation only needs frame i's
+ * accumulated history, and the plan alternates two sets of the per-frame
+ * buffers it writes (tmp_data, reprojected positions, accept mask, fitter
+ * noise table).  The first such call allocates that second set (about 40 B
+ * per pixel).  The buffers io[] points to must not be written while the
+ * call's work runs.  The fused pipeline, and any call while stage profiling
+ * is on, runs the frames one after another on `stream`. */
 int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io,
                         const float* prev_frame_camera_matrices,
                         const float* pixel_offsets, void* stream);
