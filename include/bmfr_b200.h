@@ -283,8 +283,8 @@ int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io,
  * joined back into `stream`: the accumulation only needs frame i's
  * accumulated history, and the plan alternates two sets of the per-frame
  * buffers it writes (tmp_data, reprojected positions, accept mask, fitter
- * noise table).  The first such call allocates that second set (about 40 B
- * per pixel).  The buffers io[] points to must not be written while the
+ * noise table).  The first such call allocates that second set (about 37 B
+ * per pixel with binary16 tmp_data).  The buffers io[] points to must not be written while the
  * call's work runs.  The fused pipeline, and any call while stage profiling
  * is on, runs the frames one after another on `stream`. */
 int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io,
