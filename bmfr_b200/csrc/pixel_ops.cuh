@@ -249,9 +249,13 @@ __device__ __forceinline__ float3 wsacc_core(const Geometry& g, int frame, float
     const float3 f = weighted_sum_px(load3(cur_p, lp), load3(cur_n, lp), weights + (size_t)gi * kFeatures * 3,
                                      mins_maxs + (size_t)gi * kScaled * 2);
     *filt = f;
+    // The accumulation writes the reprojected position and spp of every
+    // image pixel, so they are read beside the accept mask instead of after
+    // it: the history gather then waits for one round trip, not two.  With
+    // no accepted tap they go unused.
     const uint8_t acc = frame > 0 ? accept[lp] : 0;
-    const float2 pp = acc ? prev_pix[lp] : make_float2(0.f, 0.f);
-    const uint8_t spp = acc ? cur_spp[lp] : 1;
+    const float2 pp = frame > 0 ? prev_pix[lp] : make_float2(0.f, 0.f);
+    const uint8_t spp = frame > 0 ? cur_spp[lp] : 1;
     return accumulate_filtered_px(g, frame, lp, f, pp, acc, spp, second_alpha, acc_prev, load3(albedo, lp), tm);
 }
 
