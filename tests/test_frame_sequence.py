@@ -123,7 +123,9 @@ def test_sequence_equals_frame_by_frame(cuda, W, H, calls, kw):
 
 def test_sequence_between_single_frames(cuda):
     """Single-frame calls and sequences interleave on one plan: frames 0, 1-3,
-    4, 5-8 equal one call per frame, bit for bit."""
+    4, 5-8 equal one call per frame, bit for bit.  The last sequence runs
+    with stage profiling on, which keeps its frames in stream order, and
+    leaves the last frame's stage times readable."""
     import torch
     W, H = 160, 96
     sc = B.Scene(43, W, H, 12)
@@ -141,11 +143,14 @@ def test_sequence_between_single_frames(cuda):
                                    io["previous_normals"], io["previous_positions"], sc.prev_camera(lo),
                                    sc.pixel_offset(lo), result=results[lo])
         else:
+            mixed.enable_profiling(lo == 5)
             mixed.denoise_frames([_io(pool, f, results[f]) for f in range(lo, hi)],
                                  [sc.prev_camera(f) for f in range(lo, hi)], [sc.pixel_offset(f) for f in range(lo, hi)])
     torch.cuda.synchronize()
     for f in range(9):
         np.testing.assert_array_equal(results[f].cpu().numpy(), want[f], err_msg=f"frame {f}")
+    times = mixed.stage_times()
+    assert len(times) == 4 and all(v > 0 for v in times.values()), times
     mixed.close()
     one.close()
 
