@@ -405,16 +405,18 @@ __device__ __forceinline__ void taa_strip(const Geometry& g, int frame, float ta
         rgb_to_ycocg(s, ycc);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            // NaN and out-of-image entries as +-inf (fminf/fmaxf return the
-            // other operand of a NaN), so the neighbours' candidates come
-            // ready by shuffle; lanes 0 and 31, the halo columns, take their
-            // own as a neighbour and are not written.
-            const float vmn = in ? fminf(ycc[c], INFINITY) : INFINITY;
-            const float vmx = in ? fmaxf(ycc[c], -INFINITY) : -INFINITY;
+            // Out-of-image entries as NaN, which fminf/fmaxf skip (they
+            // return the other operand), so one shuffle each way serves both
+            // bounds; the pixel's own candidates turn a NaN into +-inf.
+            // Lanes 0 and 31, the halo columns, take their own as a
+            // neighbour and are not written.
+            const float v = in ? ycc[c] : __int_as_float(0x7fffffff);
+            const float vl = __shfl_up_sync(0xffffffffu, v, 1), vr = __shfl_down_sync(0xffffffffu, v, 1);
+            const float vmn = fminf(v, INFINITY), vmx = fmaxf(v, -INFINITY);
             cmn[k][c] = vmn;
             cmx[k][c] = vmx;
-            hmn[k][c] = fminf(fminf(__shfl_up_sync(0xffffffffu, vmn, 1), vmn), __shfl_down_sync(0xffffffffu, vmn, 1));
-            hmx[k][c] = fmaxf(fmaxf(__shfl_up_sync(0xffffffffu, vmx, 1), vmx), __shfl_down_sync(0xffffffffu, vmx, 1));
+            hmn[k][c] = fminf(fminf(vl, vmn), vr);
+            hmx[k][c] = fmaxf(fmaxf(vl, vmx), vr);
         }
         if (r >= 2) {
             const int up = (r - 2) % 3, mid = (r - 1) % 3, dn = k;
