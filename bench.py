@@ -225,6 +225,16 @@ def render_frames(seed, w, h, n):
     return sc, frames
 
 
+def host_threads():
+    """Host threads this process may run on.  Passed to the CPU kernels
+    explicitly: under torchrun OMP_NUM_THREADS is 1 in every rank, while the
+    CPU arms run on rank 0 alone and should use the whole host."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def cpu_kernels(kind, w, h, sc, threads=0):
     """The CPU implementations of the five kernels: "reference" = the
     reference's own OpenCL kernels compiled for the CPU (oracle/_ref, a fiber
@@ -275,13 +285,15 @@ def cpu_frames_per_s(kind, w, h, frames, sc, budget_s=12.0, min_frames=3, max_fr
 def cpu_baseline(frames, sc, ref_budget_s, port_budget_s):
     """cpu_baseline object: the reference's kernels on this host's cores when
     they are built, else the port; the port's figure rides along."""
-    cores = os.cpu_count()
-    fps_p, n_p, dt_p, st_p = cpu_frames_per_s("port", WIDTH, HEIGHT, frames, sc, budget_s=port_budget_s)
+    cores = host_threads()
+    fps_p, n_p, dt_p, st_p = cpu_frames_per_s("port", WIDTH, HEIGHT, frames, sc, budget_s=port_budget_s,
+                                              threads=cores)
     port = {"value": fps_p, "unit": "frames/s", "cores": cores, "kind": "port",
             "sample": f"{n_p} consecutive 1280x720 frames of the oracle pipeline ({dt_p:.1f} s)", "stages_ms": st_p}
     if not reference_available():
         return port
-    fps, n, dt, st = cpu_frames_per_s("reference", WIDTH, HEIGHT, frames, sc, budget_s=ref_budget_s)
+    fps, n, dt, st = cpu_frames_per_s("reference", WIDTH, HEIGHT, frames, sc, budget_s=ref_budget_s,
+                                      threads=cores)
     return {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
             "sample": f"{n} consecutive 1280x720 frames of the reference's OpenCL kernels compiled for the CPU "
                       f"(oracle/_ref), OpenMP over {cores} threads ({dt:.1f} s)",
@@ -295,12 +307,13 @@ def run_reference(args, world, rank):
     are not built."""
     if rank != 0:
         return
-    cores = os.cpu_count()
+    cores = host_threads()
     kind = "reference" if reference_available() else "port"
     warm = min(max(args.warmup, 1), 3)
     sc, frames = render_frames(SEED, WIDTH, HEIGHT, min(FRAMES, args.steps + warm + 1))
     fps, n, dt, stages = cpu_frames_per_s(kind, WIDTH, HEIGHT, frames, sc, budget_s=90.0,
-                                          min_frames=min(3, args.steps), max_frames=args.steps, warmup=warm)
+                                          min_frames=min(3, args.steps), max_frames=args.steps, warmup=warm,
+                                          threads=cores)
     what = ("the reference's OpenCL kernels (opencl/bmfr.cl) compiled for the CPU, a fiber per work-item "
             "at the fitter's barriers" if kind == "reference" else "the oracle port of the reference's kernels")
     sample = (f"{n} of {args.steps} requested full 1280x720 frames (90 s budget) of {what}, "
@@ -318,7 +331,7 @@ def run_reference(args, world, rank):
     }
     if kind == "reference":
         fps_p, n_p, dt_p, st_p = cpu_frames_per_s("port", WIDTH, HEIGHT, frames, sc, budget_s=20.0,
-                                                  max_frames=args.steps, warmup=warm)
+                                                  max_frames=args.steps, warmup=warm, threads=cores)
         line["port"] = {"value": fps_p, "unit": "frames/s", "cores": cores, "kind": "port", "frames": n_p,
                         "stages_ms": st_p,
                         "note": "the oracle restatement: bit-identical outputs, one loop per kernel"}
