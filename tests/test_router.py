@@ -197,7 +197,9 @@ def test_bench_launches_one_rank_per_gpu_and_checks_the_count():
 
 def test_bench_reference_arm_as_two_ranks():
     """`bench.py --impl reference --gpus 2` starts two ranks itself; rank 0
-    alone runs the CPU reference and prints one line, the other exits 0."""
+    alone runs the CPU reference and prints one line, the other exits 0.
+    torchrun sets OMP_NUM_THREADS=1 in every rank, so the arm passes its
+    thread count to the CPU kernels itself: all the host's threads."""
     import json
     import subprocess
     env = dict(os.environ)
@@ -209,3 +211,4 @@ def test_bench_reference_arm_as_two_ranks():
     assert len(lines) == 1, r.stdout
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["cpu_baseline"]["cores"] == len(os.sched_getaffinity(0))
