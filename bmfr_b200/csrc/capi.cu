@@ -684,6 +684,14 @@ int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io, con
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s, plan->ev_entry, 0);
         if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: entry");
     }
+    // On an error part way through, whatever was queued on the two streams
+    // is still ordered before the caller's later work (best effort: the
+    // error being returned is the one that counts).
+    auto join_on_error = [&]() {
+        if (!overlap) return;
+        if (cudaEventRecord(plan->ev_exit, s) == cudaSuccess) cudaStreamWaitEvent(caller, plan->ev_exit, 0);
+        if (cudaEventRecord(plan->ev_entry, sa) == cudaSuccess) cudaStreamWaitEvent(caller, plan->ev_entry, 0);
+    };
     for (int i = 0; i < count; ++i) {
         const bmfr_frame_io& x = io[i];
         const int f = plan->frame;
@@ -692,12 +700,17 @@ int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io, con
         // set, and its accumulation precedes this one on the same stream.
         if (overlap && i >= 2) {
             cudaError_t e = cudaStreamWaitEvent(sa, plan->ev_frame_done[(f - 2) % 3], 0);
-            if (e != cudaSuccess) return cuda_fail(e, "denoise_frames: frame order");
+            if (e != cudaSuccess) {
+                join_on_error();
+                return cuda_fail(e, "denoise_frames: frame order");
+            }
         }
         if (int st = run_frame(plan, x.albedo, x.normals, x.previous_normals, x.positions, x.previous_positions,
                                x.noisy, x.result, prev_frame_camera_matrices + 16 * (size_t)i,
-                               pixel_offsets + 2 * (size_t)i, s, sa, overlap ? (f & 1) : 0))
+                               pixel_offsets + 2 * (size_t)i, s, sa, overlap ? (f & 1) : 0)) {
+            join_on_error();
             return st;
+        }
     }
     if (overlap) {
         // Every accumulation has been waited for on the frame stream; its
