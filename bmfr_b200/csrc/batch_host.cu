@@ -330,10 +330,14 @@ cudaError_t launch_staged_step(bmfr_batch* b, const bmfr::BatchStepDesc& d, cuda
             e = bmfr::launch_taa(g, f, J.taa_alpha, fb.prev_pix, fb.tone_mapped, J.result_hist, J.result_prev,
                                  J.result_out, half_hist, ws);
     }
-    for (int w = 0; w < kStepWorkers && e == cudaSuccess; ++w) {
+    // Every worker that took work joins back to `s`, after an error too, so
+    // what was queued stays ordered before the caller's later work; the
+    // first error is the one returned.
+    for (int w = 0; w < kStepWorkers; ++w) {
         if (!used[w]) continue;
-        e = cudaEventRecord(b->join[w], b->workers[w]);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->join[w], 0);
+        cudaError_t ej = cudaEventRecord(b->join[w], b->workers[w]);
+        if (ej == cudaSuccess) ej = cudaStreamWaitEvent(s, b->join[w], 0);
+        if (e == cudaSuccess) e = ej;
     }
     return e;
 }
