@@ -38,7 +38,8 @@ struct Request {
 };
 
 struct StepRecord {
-    cudaEvent_t done;
+    cudaEvent_t done = nullptr;   // null if the step's event could not be made
+    bool last = false;            // the scheduler's final record: the completion thread ends
     std::vector<uint64_t> requests;
     std::vector<int> streams;
     std::vector<Clock::time_point> arrivals;
@@ -130,9 +131,12 @@ void schedule_loop(bmfr_server* s) {
             std::memcpy(&offs[2 * i], take[i].offset, sizeof take[i].offset);
         }
         StepRecord rec;
-        cudaEventCreateWithFlags(&rec.done, cudaEventDisableTiming);
-        int st;
-        {
+        int st = BMFR_OK;
+        if (cudaEventCreateWithFlags(&rec.done, cudaEventDisableTiming) != cudaSuccess) {
+            rec.done = nullptr;
+            st = fail(BMFR_E_CUDA, "server: creating a step's event failed");
+        }
+        if (st == BMFR_OK) {
             std::lock_guard<std::mutex> blk(s->batch_mu);
             st = bmfr_batch_step(s->batch, n, slots.data(), io.data(), mats.data(), offs.data(), s->stream);
         }
@@ -162,7 +166,7 @@ void schedule_loop(bmfr_server* s) {
     {
         std::lock_guard<std::mutex> lk(s->step_mu);
         StepRecord sentinel;
-        sentinel.done = nullptr;
+        sentinel.last = true;
         s->steps_in_flight.push_back(std::move(sentinel));
     }
     s->cv_steps.notify_one();
@@ -180,10 +184,14 @@ void complete_loop(bmfr_server* s) {
             rec = std::move(s->steps_in_flight.front());
             s->steps_in_flight.pop_front();
         }
-        if (!rec.done) break;
-        cudaEventSynchronize(rec.done);
+        if (rec.last) break;
+        if (rec.done) {
+            cudaEventSynchronize(rec.done);
+        } else {
+            cudaStreamSynchronize(s->stream);   // no event: wait for everything queued so far
+        }
         const Clock::time_point t = Clock::now();
-        cudaEventDestroy(rec.done);
+        if (rec.done) cudaEventDestroy(rec.done);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             for (size_t i = 0; i < rec.requests.size(); ++i) {
