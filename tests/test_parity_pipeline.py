@@ -43,8 +43,11 @@ def device_array(ptr, shape, dtype):
 # 1280x720: 984 blocks, more than the persistent fitter's CTAs, so each CTA
 # fits several blocks through both tile buffers and both barrier phases.
 # 1920x1080 and 3840x2160: the precision and many-stream workloads' sizes.
+# 32x32 and 47x63: the smallest accepted images, whose mirrored margin
+# reaches the last index mirror() serves (bmfr.cl:209-216), over all 16
+# block offsets.
 @pytest.mark.parametrize("W,H,frames", [(128, 96, 17), (256, 256, 8), (197, 131, 5), (1280, 720, 3),
-                                        (1920, 1080, 2), (3840, 2160, 1)])
+                                        (1920, 1080, 2), (3840, 2160, 1), (32, 32, 17), (47, 63, 17)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
     import torch
     sc = B.Scene(21, W, H, 12)
@@ -120,8 +123,13 @@ def test_kept_intermediates_change_no_output(cuda, half_history):
 def test_pipeline_rejects_bad_arguments(cuda):
     with pytest.raises(B.BmfrError):
         B.Plan(16, 16)
-    with pytest.raises(B.BmfrError):
-        B.Plan(33, 64)   # too small for the mirrored margin
+    # Widths 33..46 leave the mirrored margin beyond one image size; 32 and
+    # 47 are the limits on either side (the same rule for heights).
+    for w, h in ((33, 64), (46, 64), (64, 46)):
+        with pytest.raises(B.BmfrError):
+            B.Plan(w, h)
+    for w, h in ((32, 64), (47, 64), (64, 47)):
+        B.Plan(w, h).close()
     plan = B.Plan(64, 64)
     with pytest.raises(ValueError):
         plan.denoise_frame(np.zeros(15), np.zeros(2))

@@ -44,7 +44,7 @@ def assert_close(got, want, what, rtol=RTOL, floor=FLOOR):
 
 
 # 1280x720: 984 blocks, more than the persistent fitter's CTAs.
-SIZES = [(64, 64), (100, 70), (256, 256), (1280, 720)]
+SIZES = [(64, 64), (100, 70), (256, 256), (1280, 720), (32, 32), (47, 63)]   # the last two: smallest accepted
 
 
 @pytest.mark.parametrize("W,H", SIZES)

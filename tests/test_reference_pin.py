@@ -118,12 +118,15 @@ needs_ref = pytest.mark.skipif(not REF.available(), reason="reference kernel sou
 
 
 @needs_ref
-@pytest.mark.parametrize("W,H,frames,half", [(128, 96, 17, True), (200, 120, 4, True), (160, 96, 4, False)])
+@pytest.mark.parametrize("W,H,frames,half", [(128, 96, 17, True), (200, 120, 4, True), (160, 96, 4, False),
+                                             (32, 32, 17, True), (47, 63, 17, True)])
 def test_oracle_matches_compiled_reference(W, H, frames, half):
     """Frame loops over the oracle and over the reference's kernels: every
     intermediate buffer identical, tmp_data after the fitter included (the
     QR intermediates the reference leaves there).  17 frames cover all 16
-    block offsets."""
+    block offsets.  32x32 and 47x63 are the smallest images whose mirrored
+    margin stays within one image size (mirror, bmfr.cl:209-216): there the
+    margin reaches the last valid index."""
     import bmfr_b200 as B
     sc = B.Scene(21, W, H, 12)
     kw = dict(position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared,
