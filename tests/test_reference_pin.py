@@ -119,7 +119,7 @@ needs_ref = pytest.mark.skipif(not REF.available(), reason="reference kernel sou
 
 @needs_ref
 @pytest.mark.parametrize("W,H,frames,half", [(128, 96, 17, True), (200, 120, 4, True), (160, 96, 4, False),
-                                             (32, 32, 17, True), (47, 63, 17, True)])
+                                             (32, 32, 17, True), (47, 63, 17, True), (64, 48, 17, False)])
 def test_oracle_matches_compiled_reference(W, H, frames, half):
     """Frame loops over the oracle and over the reference's kernels: every
     intermediate buffer identical, tmp_data after the fitter included (the
