@@ -49,12 +49,24 @@ def device_array(ptr, shape, dtype):
 @pytest.mark.parametrize("W,H,frames", [(128, 96, 17), (256, 256, 8), (197, 131, 5), (1280, 720, 3),
                                         (1920, 1080, 2), (3840, 2160, 1), (32, 32, 17), (47, 63, 17)])
 def test_pipeline_matches_oracle(cuda, pipeline, W, H, frames):
+    _pipeline_parity(pipeline, W, H, frames, use_half=1)
+
+
+# float32 tmp_data (USE_HALF_PRECISION_IN_TMP_DATA=0, opencl/bmfr.cpp:88):
+# the fitter's one-dimensional bulk copy and float tile, over all 16 block
+# offsets.
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
+def test_pipeline_with_float_tmp_data_matches_oracle(cuda, pipeline):
+    _pipeline_parity(pipeline, 64, 48, 17, use_half=0)
+
+
+def _pipeline_parity(pipeline, W, H, frames, use_half):
     import torch
     sc = B.Scene(21, W, H, 12)
     plan = B.Plan(W, H, pipeline=pipeline, position_limit_squared=sc.position_limit_squared,
-                  normal_limit_squared=sc.normal_limit_squared)
+                  normal_limit_squared=sc.normal_limit_squared, use_half_precision_in_tmp_data=use_half)
     plan.keep_intermediates(True)   # the tone-mapped frame is checked below
-    ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared))
+    ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared, use_half=bool(use_half)))
     for f in range(frames):
         d = sc.render(f)
         plan.upload_frame(d["albedo"], d["normals"], d["positions"], d["noisy"])
