@@ -55,19 +55,21 @@ def _pick(rng, n, k):
     return rng.choice(n, size=k, replace=False)
 
 
-def stage_inputs():
-    """One frame's adversarial inputs for every stage (dict of arrays)."""
+def stage_inputs(seed=STAGE_SEED, frame=STAGE_FRAME):
+    """One frame's adversarial inputs for every stage (dict of arrays).  The
+    defaults give the committed fixture; other seeds and frames (>= 1) give
+    further cases of the same kinds, frame % 16 picking the block offset."""
     import bmfr_b200 as B
     w, h = STAGE_SIZE
     px = w * h
     mw, mh, blocks = geometry(w, h)
-    rng = np.random.default_rng(STAGE_SEED)
-    sc = B.Scene(STAGE_SEED, w, h, 16)
-    prev, cur = sc.render(STAGE_FRAME - 1), sc.render(STAGE_FRAME)
+    rng = np.random.default_rng(seed)
+    sc = B.Scene(seed, w, h, 16)
+    prev, cur = sc.render(frame - 1), sc.render(frame)
     d = {"limits": np.array([sc.position_limit_squared, sc.normal_limit_squared], np.float32),
-         "frame": np.array([STAGE_FRAME], np.int32),
-         "matrix": sc.prev_camera(STAGE_FRAME).astype(np.float32),
-         "offset": sc.pixel_offset(STAGE_FRAME).astype(np.float32)}
+         "frame": np.array([frame], np.int32),
+         "matrix": sc.prev_camera(frame).astype(np.float32),
+         "offset": sc.pixel_offset(frame).astype(np.float32)}
 
     # accumulate_noisy_data.  The extreme values sit in the top 12 rows only:
     # one value clamped to 65504 overflows the binary16 QR of its whole block

@@ -157,6 +157,61 @@ def test_stage_fixture_is_the_reference_output():
             same(v, g[name], name)
 
 
+def stage_chain(k, d, seed):
+    """The five stages of kernel set `k` on stage inputs `d`
+    (cases.stage_inputs), each fed by the previous stage's outputs and the
+    fitter by the accumulation's tmp_data with the adversarial blocks
+    written in; returns every output."""
+    import cases
+    w, h = cases.STAGE_SIZE
+    f = int(d["frame"][0])
+    o = k(w, h, float(d["limits"][0]), float(d["limits"][1]))
+    out = {}
+    pp = np.zeros((h, w, 2), np.float32)
+    acc = np.zeros((h, w), np.uint8)
+    spp = np.zeros((h, w), np.uint8)
+    noisy = d["cur_noisy"].copy()
+    tmp = o.new_tmp()
+    o.accumulate_noisy_data(pp, acc, d["cur_normals"], d["prev_normals"], d["cur_positions"], d["prev_positions"],
+                            noisy, d["prev_noisy"], d["prev_spp"], spp, tmp, d["matrix"], d["offset"], f)
+    out.update(prev_pix=pp, accept=acc, spp=spp, noisy=noisy, tmp=tmp.copy())
+    t = cases.patch_fit_blocks(tmp, d["fit_blocks"], rng_seed=seed)
+    weights = np.zeros(o.blocks * 30, np.float32)
+    mm = np.zeros(o.blocks * 12, np.float32)
+    o.fitter(weights, mm, t, f)
+    out.update(weights=weights, mins_maxs=mm, tmp_after_fit=t)
+    filt = np.zeros((h, w, 3), np.float32)
+    o.weighted_sum(weights, mm, filt, d["cur_normals"], d["cur_positions"], f)
+    tone = np.zeros((h, w, 3), np.float32)
+    acc_cur = np.zeros((h, w, 3), np.float32)
+    o.accumulate_filtered_data(filt, d["prev_pix"], d["accept"], d["albedo"], tone, d["cur_spp"], d["acc_prev"],
+                               acc_cur, f)
+    res = np.zeros((h, w, 3), np.float32)
+    o.taa(d["taa_prev_pix"], tone, res, d["taa_prev"], f)
+    out.update(filtered=filt, tone_mapped=tone, accumulated=acc_cur, result=res)
+    return out
+
+
+@needs_ref
+@pytest.mark.parametrize("offset", range(16))
+def test_oracle_matches_compiled_reference_on_edge_inputs(offset):
+    """The stage fixture's kinds of edge inputs (NaN, infinities, values
+    beyond binary16, spp 0 and 255, constant, zero and +-65504 blocks,
+    history positions on and beyond every edge) drawn anew for each of the
+    16 block offsets (frame 16 + offset), through the oracle and the
+    reference's compiled kernels: every output equal bit for bit."""
+    import cases
+    seed = 1000 + offset
+    d = cases.stage_inputs(seed=seed, frame=16 + offset)
+    a = stage_chain(Oracle, d, seed)
+    b = stage_chain(REF.RefKernels, d, seed)
+    for name in a:   # in stage order: the first difference names its stage
+        same(a[name], b[name], f"{name} (block offset {offset})")
+    # The case reaches the edge branches it is drawn for.
+    assert np.isnan(b["weights"]).any() and (b["spp"] == 255).any() and np.isnan(b["prev_pix"]).any()
+    assert 0.2 < (b["accept"] > 0).mean() < 1.0
+
+
 def test_prepare_rules_fail_loudly():
     """The source preparation rewrites exactly the constructs it expects."""
     sys.path.insert(0, str(Path(REF.__file__).resolve().parent / "ref_cl"))
