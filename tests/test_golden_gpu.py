@@ -71,8 +71,59 @@ def test_plan_pipeline_matches_reference_fixture(cuda, pipeline, fixture, use_ha
 
 
 def test_dropin_stages_match_reference_edge_fixture(cuda):
+    _check_dropin_stages(cuda, np.load(GOLDEN / "ref_stages.npz"))
+
+
+def _oracle_stage_case(seed, frame):
+    """The stage fixture's kinds of edge inputs drawn for (seed, frame)
+    (tests/golden/cases.py) with the oracle's output of every stage, under
+    the fixture's names.  The oracle equals the compiled reference bit for
+    bit on these same cases (tests/test_reference_pin.py)."""
+    import sys
+    if str(GOLDEN) not in sys.path:
+        sys.path.insert(0, str(GOLDEN))
+    import cases
+    from oracle.oracle import Oracle
+    d = cases.stage_inputs(seed=seed, frame=frame)
+    w, h = cases.STAGE_SIZE
+    o = Oracle(w, h, float(d["limits"][0]), float(d["limits"][1]))
+    g = {f"in_{k}": v for k, v in d.items()}
+    pp = np.zeros((h, w, 2), np.float32)
+    acc = np.zeros((h, w), np.uint8)
+    spp = np.zeros((h, w), np.uint8)
+    noisy = d["cur_noisy"].copy()
+    tmp = o.new_tmp()
+    o.accumulate_noisy_data(pp, acc, d["cur_normals"], d["prev_normals"], d["cur_positions"], d["prev_positions"],
+                            noisy, d["prev_noisy"], d["prev_spp"], spp, tmp, d["matrix"], d["offset"], frame)
+    g.update(out_acc_prev_pix=pp, out_acc_accept=acc, out_acc_spp=spp, out_acc_noisy=noisy, out_acc_tmp=tmp.copy())
+    fit_in = cases.patch_fit_blocks(tmp.copy(), d["fit_blocks"], rng_seed=seed)
+    weights = np.zeros(o.blocks * 30, np.float32)
+    mm = np.zeros(o.blocks * 12, np.float32)
+    o.fitter(weights, mm, fit_in.copy(), frame)
+    g.update(in_fit_tmp=fit_in, out_fit_weights=weights, out_fit_mins_maxs=mm)
+    filt = np.zeros((h, w, 3), np.float32)
+    o.weighted_sum(weights, mm, filt, d["cur_normals"], d["cur_positions"], frame)
+    tone = np.zeros((h, w, 3), np.float32)
+    acc_cur = np.zeros((h, w, 3), np.float32)
+    o.accumulate_filtered_data(filt, d["prev_pix"], d["accept"], d["albedo"], tone, d["cur_spp"], d["acc_prev"],
+                               acc_cur, frame)
+    res = np.zeros((h, w, 3), np.float32)
+    o.taa(d["taa_prev_pix"], tone, res, d["taa_prev"], frame)
+    g.update(out_ws_filtered=filt, out_af_tone_mapped=tone, out_af_accumulated=acc_cur, out_taa_result=res)
+    return g
+
+
+@pytest.mark.parametrize("offset", range(16))
+def test_dropin_stages_match_oracle_on_edge_inputs(cuda, offset):
+    """Edge inputs drawn anew for each of the 16 block offsets (frame
+    16 + offset) through the five drop-in entry points."""
+    _check_dropin_stages(cuda, _oracle_stage_case(1000 + offset, 16 + offset))
+
+
+def _check_dropin_stages(cuda, g):
+    """The five drop-in entry points on stage inputs `g`, each against the
+    expected output of its stage under the stage fixture's names."""
     import torch
-    g = np.load(GOLDEN / "ref_stages.npz")
     H, W = g["in_albedo"].shape[:2]
     px = W * H
     f = int(g["in_frame"][0])
