@@ -151,3 +151,21 @@ def patch_fit_blocks(tmp: np.ndarray, blocks, rng_seed=STAGE_SEED):
     t[b1] = 0
     t[b2, 1:10] = rng.choice(np.array([-65504.0, 65504.0, 0.0], np.float32), (9, 1024)).astype(t.dtype)
     return tmp
+
+
+def edge_frame(d, rng, w, h):
+    """A scene frame with a few edge values written in at random pixels:
+    NaN, +-inf and beyond-binary16 colours, NaN and out-of-range positions
+    (the stage fixture's kinds, here carried through the histories of the
+    following frames)."""
+    px = w * h
+    noisy = d["noisy"].reshape(px, 3).copy()
+    pos = d["positions"].reshape(px, 3).copy()
+    idx = rng.choice(px, size=8, replace=False)
+    noisy[idx[:2]] = np.nan
+    noisy[idx[2]] = np.inf
+    noisy[idx[3]] = -np.inf
+    noisy[idx[4:6]] = rng.uniform(7e4, 1e6, (2, 3))
+    pos[idx[6]] = np.nan
+    pos[idx[7]] = rng.uniform(260.0, 400.0, 3)
+    return dict(d, noisy=noisy.reshape(h, w, 3), positions=pos.reshape(h, w, 3))

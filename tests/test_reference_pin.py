@@ -145,6 +145,42 @@ def test_oracle_matches_compiled_reference(W, H, frames, half):
 
 
 @needs_ref
+@pytest.mark.parametrize("half", [True, False])
+def test_oracle_matches_compiled_reference_with_edge_frames(half):
+    """17 consecutive frames (all 16 block offsets) of the scene with edge
+    values written into every fourth frame, so NaN and overflowing values
+    pass through the spp, colour and TAA histories: every buffer of the
+    oracle and of the compiled reference equal bit for bit, frame after
+    frame."""
+    import bmfr_b200 as B
+    import cases
+    W, H = 64, 48
+    sc = B.Scene(41, W, H, 12)
+    rng = np.random.default_rng(41)
+    kw = dict(position_limit_squared=sc.position_limit_squared, normal_limit_squared=sc.normal_limit_squared,
+              use_half=half)
+    po, pr = OraclePipeline(Oracle(W, H, **kw)), OraclePipeline(REF.RefKernels(W, H, **kw))
+    nan_hist = False
+    for f in range(17):
+        d = sc.render(f)
+        if f % 4 == 1:   # edge values every fourth frame; the histories carry them between
+            d = cases.edge_frame(d, rng, W, H)
+        args = (d["albedo"], d["normals"], d["positions"], d["noisy"], sc.prev_camera(f), sc.pixel_offset(f))
+        same(po.step(*args), pr.step(*args), f"result {f}")
+        c = f & 1
+        for name in ("tmp_after_accumulate", "tmp", "prev_pix", "accept", "mins_maxs", "weights", "filtered",
+                     "tone_mapped"):
+            same(getattr(po, name), getattr(pr, name), f"{name} {f}")
+        for name in ("spp", "noisy", "acc", "result"):
+            same(getattr(po, name)[c], getattr(pr, name)[c], f"{name} {f}")
+        nan_hist = nan_hist or bool(np.isnan(pr.acc[c]).any())
+    # NaN reached the accumulated filtered history (whose bilinear reads
+    # spread it, as the reference's do), and the last frame still has lit
+    # pixels of the scene.
+    assert nan_hist and (pr.result[16 & 1] > 0).mean() > 0.05
+
+
+@needs_ref
 def test_stage_fixture_is_the_reference_output():
     """The committed edge-case fixture is what the compiled reference gives
     on its inputs today (the fixture and the runner agree)."""
