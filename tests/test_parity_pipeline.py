@@ -1,5 +1,7 @@
 """End-to-end parity of the plan-managed frame pipeline (staged and fused
 forms) with the oracle's frame loop, through host-buffer uploads."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -60,15 +62,33 @@ def test_pipeline_with_float_tmp_data_matches_oracle(cuda, pipeline):
     _pipeline_parity(pipeline, 64, 48, 17, use_half=0)
 
 
-def _pipeline_parity(pipeline, W, H, frames, use_half):
+# Edge values (NaN, +-inf, beyond binary16; NaN and out-of-range positions)
+# written into every fourth frame, carried by the histories in between: the
+# case the oracle is pinned on against the compiled reference
+# (tests/test_reference_pin.py, the same scene and draws).
+@pytest.mark.parametrize("pipeline", [B.PIPELINE_STAGED, B.PIPELINE_FUSED])
+def test_pipeline_with_edge_frames_matches_oracle(cuda, pipeline):
+    _pipeline_parity(pipeline, 64, 48, 17, use_half=1, scene_seed=41, edge_seed=41)
+
+
+def _pipeline_parity(pipeline, W, H, frames, use_half, scene_seed=21, edge_seed=None):
     import torch
-    sc = B.Scene(21, W, H, 12)
+    sc = B.Scene(scene_seed, W, H, 12)
+    if edge_seed is not None:
+        import sys
+        golden = str(Path(__file__).resolve().parent / "golden")
+        if golden not in sys.path:
+            sys.path.insert(0, golden)
+        import cases
+        rng = np.random.default_rng(edge_seed)
     plan = B.Plan(W, H, pipeline=pipeline, position_limit_squared=sc.position_limit_squared,
                   normal_limit_squared=sc.normal_limit_squared, use_half_precision_in_tmp_data=use_half)
     plan.keep_intermediates(True)   # the tone-mapped frame is checked below
     ref = OraclePipeline(Oracle(W, H, sc.position_limit_squared, sc.normal_limit_squared, use_half=bool(use_half)))
     for f in range(frames):
         d = sc.render(f)
+        if edge_seed is not None and f % 4 == 1:
+            d = cases.edge_frame(d, rng, W, H)
         plan.upload_frame(d["albedo"], d["normals"], d["positions"], d["noisy"])
         plan.denoise_frame(sc.prev_camera(f), sc.pixel_offset(f))
         got = plan.download_result()
