@@ -286,7 +286,10 @@ int bmfr_denoise_frame_io(bmfr_plan* plan, const bmfr_frame_io* io,
  * noise table).  The first such call allocates that second set (about 37 B
  * per pixel with binary16 tmp_data).  The buffers io[] points to must not be written while the
  * call's work runs.  The fused pipeline, and any call while stage profiling
- * is on, runs the frames one after another on `stream`. */
+ * is on, runs the frames one after another on `stream`.  Every frame's
+ * arguments are checked before the first is queued; a CUDA error part way
+ * through returns its status, and what was already queued on the plan's two
+ * streams is still joined back into `stream`. */
 int bmfr_denoise_frames(bmfr_plan* plan, int count, const bmfr_frame_io* io,
                         const float* prev_frame_camera_matrices,
                         const float* pixel_offsets, void* stream);
